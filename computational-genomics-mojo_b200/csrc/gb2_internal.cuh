@@ -1,0 +1,93 @@
+// gb2_internal.cuh -- shared declarations of libgenomics_b200 (not installed).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "genomics_b200.h"
+
+namespace gb2 {
+
+// Device view of one SequenceBatch side of a pair list.
+struct SeqView {
+    const uint64_t *packed;  // packed words resident on the device
+    const int64_t *offsets;  // word offset of each sequence (SequenceBatch.offsets)
+    const int64_t *lengths;  // bases of each sequence (SequenceBatch.lengths)
+    int64_t word_base;       // offsets[i] - word_base indexes `packed`
+    int64_t n_words;         // words in `packed` (reads are clamped to it)
+};
+
+// Which pairs a launch processes: queue[start .. start+n) of pair indices
+// (queue == nullptr: pairs [0, n)).  When seg != nullptr the device array
+// seg[0..1] = [start, end) overrides n (set by the bucketing kernels).
+// counter != nullptr hands out queue slots dynamically (atomics); it must
+// be zero at launch.
+struct PairList {
+    const int32_t *queue;
+    int64_t n;
+    const int64_t *seg;
+    int *counter;
+};
+
+// Loads the 64-bit window of 32 bases starting at base `pos` of a sequence
+// whose first word is `word0` (global word index); words outside
+// [0, n_words) read as the nearest valid word, so any pos is safe to load
+// (callers mask or ignore bases outside the sequence).
+__device__ __forceinline__ uint64_t load_window64(const uint64_t *__restrict__ packed,
+                                                  int64_t n_words, int64_t word0,
+                                                  int64_t pos)
+{
+    int64_t w = word0 + (pos >> 5);
+    int sh = (int)(pos & 31) * 2;
+    int64_t w0 = w < 0 ? 0 : (w >= n_words ? n_words - 1 : w);
+    int64_t w1 = w + 1 < 0 ? 0 : (w + 1 >= n_words ? n_words - 1 : w + 1);
+    uint64_t a = __ldg(packed + w0);
+    uint64_t b = __ldg(packed + w1);
+    return sh ? ((a << sh) | (b >> (64 - sh))) : a;
+}
+
+// Base at position pos (MSB-first), genomics/core/dna.mojo:96-100.
+// Resolves a PairList on the device: returns the queue base and sets n.
+__device__ __forceinline__ const int32_t *pairs_resolve(const PairList &pl, int64_t &n)
+{
+    if (pl.seg) {
+        const int64_t s0 = pl.seg[0];
+        n = pl.seg[1] - s0;
+        return pl.queue + s0;
+    }
+    n = pl.n;
+    return pl.queue;
+}
+
+}  // namespace gb2
+
+// Launch helpers implemented in the kernel translation units.
+namespace gb2 {
+
+struct SwParams {
+    int32_t match, mismatch, go, ge;
+};
+
+// Smith-Waterman launch over a list of pair indices (queue == nullptr means
+// pairs [0, n)).  `bands` (device, may be nullptr) overrides `band`.
+// band_class: 16, 32, 64, 128 for the register kernels, 0 for the literal
+// per-pair kernel.  Returns a cudaError_t.
+cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParams p,
+                      int32_t band, const int32_t *bands, PairList pl, gb2_sw_result *out,
+                      int64_t *scratch, int64_t scratch_stride, int grid, cudaStream_t st);
+
+// Pairs per 128-thread block, and resident blocks per SM, of a kernel variant.
+int sw_pairs_per_block(int band_class, int variant);
+int sw_blocks_per_sm(int band_class, int variant);
+
+struct WfaParams {
+    int32_t x, o, e, max_error;
+};
+
+cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList pl, int32_t *out,
+                       int32_t *scratch, int64_t slot_width, int grid, int *err_flag,
+                       int64_t *work, cudaStream_t st);
+
+cudaError_t launch_int_peak(int kind, int grid, int block, int iters, uint32_t *sink,
+                            cudaStream_t st);
+
+}  // namespace gb2

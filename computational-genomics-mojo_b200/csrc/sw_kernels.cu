@@ -1,0 +1,393 @@
+// sw_kernels.cu -- banded Smith-Waterman on sm_100a.
+//
+// Computes smith_waterman_banded (genomics/cpu/align_cpu.mojo:229-309)
+// bit-exactly: score plus the first maximum cell in row-major order.
+//
+// Band coordinates: row qi (query position), column j in [0, 2B],
+// ri = qi - B + j.  Cell (qi, j) reads diag (qi-1, j), up (qi-1, j+1) and
+// left (qi, j-1) (align_cpu.mojo:277-279); E extends along the row from the
+// left cell's E and opens from up (:282-283); F opens from the left H with
+// no extension (:287).
+//
+// Register kernel (sw_band_kernel<B, G, K>): G lanes of a warp own one pair;
+// lane l owns band columns [l*K, l*K + K) and keeps their H values in
+// registers.  Lane l processes row t - l at step t: its first column takes
+// the left neighbour's last column of the same row (computed by lane l-1 one
+// step earlier, passed by warp shuffle) and its last column takes as "up"
+// the right neighbour's first column of the previous row (computed by lane
+// l+1 in the first phase of the same step, passed by shuffle).  With G == 1
+// a thread owns the whole band row and no shuffles run.
+//
+// Exactness of the register kernel rests on three facts, valid when
+// gap_extend <= 0, gap_open + gap_extend <= 0 and mismatch <= 0 (the host
+// checks these and otherwise uses the literal kernel):
+//  1. E only influences H through max(E, 0), and with gap_extend <= 0 a
+//     non-positive E never becomes positive along the row, so carrying
+//     E+ = max(E, 0) reproduces every H.  The reference's -1000000 start of
+//     the E chain at j == 0 and the zero E of a skipped cell (:282) both
+//     become E+ = 0 on the left boundary.
+//  2. Cells left of the reference start (ri < 0) are skipped (zero) in the
+//     reference; giving them a never-matching base makes the recurrence
+//     produce exactly zero there, so no per-cell masking is needed.
+//  3. Cells past the reference end (ri >= rlen) or past the query end never
+//     feed a cell inside the matrix (every dependency has column <= ri and
+//     row <= qi), so they are computed but excluded from the maximum.
+// Padding columns past 2B in the last lane are forced to zero so column 2B
+// sees the out-of-band "up" value 0 (:278).
+#include "gb2_internal.cuh"
+
+namespace gb2 {
+
+__device__ __forceinline__ void sw_cell(int32_t hdiag, int32_t hup, int32_t hleft,
+                                        int32_t eleft, int32_t sub, int32_t goe,
+                                        int32_t ge, int32_t &hn, int32_t &en)
+{
+    // E+ = max(E_left + ge, H_up + go + ge, 0)
+    en = __viaddmax_s32_relu(hup, goe, eleft + ge);
+    // H = max(H_diag + sub, E+, H_left + go + ge, 0)
+    hn = __viaddmax_s32_relu(hleft, goe, __viaddmax_s32(hdiag, sub, en));
+}
+
+// Writes the result of one pair from the group's packed best key.
+__device__ __forceinline__ void sw_store(gb2_sw_result *out, int64_t pi, uint64_t key, int B)
+{
+    gb2_sw_result res;
+    if (key == 0) {
+        res.score = 0;
+        res.query_end = 0;
+        res.ref_end = 0;
+    } else {
+        int32_t best = (int32_t)(key >> 42);
+        int32_t bq = 0x1FFFFF - (int32_t)((key >> 21) & 0x1FFFFF);
+        int32_t bj = 0x1FFFFF - (int32_t)(key & 0x1FFFFF);
+        res.score = best;
+        res.query_end = bq;
+        res.ref_end = bq - B + bj;
+    }
+    out[pi] = res;
+}
+
+template <int B, int G, int K>
+__global__ void __launch_bounds__(128)
+sw_band_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__restrict__ out)
+{
+    int64_t n;
+    const int32_t *__restrict__ queue = pairs_resolve(pl, n);
+    int *const queue_counter = pl.counter;
+    constexpr int W = 2 * B + 1;
+    static_assert(G * K >= W, "band does not fit");
+    static_assert(G == 1 || K >= 2, "pipelined lanes need two columns");
+    static_assert(32 % G == 0, "G divides the warp");
+    constexpr int CPAD = W - (G - 1) * K;  // first padding column of the last lane
+    static_assert(CPAD >= 1 && CPAD <= K, "G is not minimal");
+    constexpr int NW = (K + 31) / 32;  // 64-bit window words per lane
+    constexpr int PAIRS_PER_WARP = 32 / G;
+
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int gw = lane / G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gw * G));
+    const int warps_per_block = blockDim.x >> 5;
+    const int64_t warp_global = (int64_t)blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+    const int64_t warps_total = (int64_t)gridDim.x * warps_per_block;
+
+    const int32_t goe = p.go + p.ge;
+    const int32_t ge = p.ge;
+    const int32_t m = p.match, mm = p.mismatch;
+
+    int64_t base = warp_global * PAIRS_PER_WARP;
+    for (;;) {
+        if (queue_counter) {
+            int64_t b0 = 0;
+            if (lane == 0)
+                b0 = atomicAdd(queue_counter, PAIRS_PER_WARP);
+            base = __shfl_sync(0xffffffffu, b0, 0);
+        }
+        if (base >= n)
+            break;
+        const int64_t slot = base + gw;
+        if (slot < n) {
+            const int64_t pi = queue ? (int64_t)queue[slot] : slot;
+            const int64_t qoff = q.offsets[pi] - q.word_base;
+            const int64_t roff = r.offsets[pi] - r.word_base;
+            const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
+
+            int32_t H[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c)
+                H[c] = 0;
+            int32_t h_in = 0, e_in = 0;
+            int32_t best = 0, bq = 0, bj = 0;
+            const int steps = qlen > 0 ? qlen + G - 1 : 0;
+            for (int t = 0; t < steps; ++t) {
+                const int qi = t - gl;
+                const bool row_live = (qi >= 0) && (qi < qlen);
+                const int64_t ri0 = (int64_t)qi - B + gl * K;
+                uint64_t eq[NW];
+                if (row_live) {
+                    const uint64_t qw = __ldg(q.packed + qoff + (qi >> 5));
+                    const uint64_t qb = (qw >> (62 - 2 * (qi & 31))) & 3u;
+                    const uint64_t qrep = qb * 0x5555555555555555ull;
+                    // NW+1 consecutive words cover the K-base window at ri0
+                    const int64_t w = roff + (ri0 >> 5);
+                    const int sh = (int)(ri0 & 31) * 2;
+                    uint64_t words[NW + 1];
+#pragma unroll
+                    for (int i = 0; i <= NW; ++i) {
+                        int64_t wi = w + i;
+                        wi = wi < 0 ? 0 : (wi >= r.n_words ? r.n_words - 1 : wi);
+                        words[i] = __ldg(r.packed + wi);
+                    }
+#pragma unroll
+                    for (int i = 0; i < NW; ++i) {
+                        const uint64_t win =
+                            sh ? ((words[i] << sh) | (words[i + 1] >> (64 - sh))) : words[i];
+                        const uint64_t x = win ^ qrep;
+                        eq[i] = ~(x | (x >> 1)) & 0x5555555555555555ull;
+                    }
+                    if (ri0 < 0) {  // columns before the reference start never match
+                        const int64_t nneg = -ri0;
+#pragma unroll
+                        for (int i = 0; i < NW; ++i) {
+                            const int64_t cnt = nneg - 32 * i;
+                            if (cnt >= 32)
+                                eq[i] = 0;
+                            else if (cnt > 0)
+                                eq[i] &= (~0ull) >> (2 * cnt);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NW; ++i)
+                        eq[i] = 0;
+                }
+
+                // phase 1: first column
+                int32_t hn, en;
+                {
+                    const int32_t sub = ((eq[0] >> 62) & 1u) ? m : mm;
+                    const int32_t hup = (K > 1) ? H[K > 1 ? 1 : 0] : 0;
+                    sw_cell(H[0], hup, h_in, e_in, sub, goe, ge, hn, en);
+                    if (CPAD == 0 && gl == G - 1)
+                        hn = 0;
+                    H[0] = hn;
+                }
+                int32_t up_next = 0;
+                if (G > 1) {
+                    up_next = __shfl_down_sync(gmask, hn, 1, G);
+                    if (gl == G - 1)
+                        up_next = 0;
+                }
+                int32_t hl = hn, el = en;
+                // phase 2: remaining columns, left to right
+#pragma unroll
+                for (int c = 1; c < K; ++c) {
+                    const int32_t sub =
+                        ((eq[c >> 5] >> (62 - 2 * (c & 31))) & 1u) ? m : mm;
+                    const int32_t hup = (c + 1 < K) ? H[c + 1 < K ? c + 1 : c] : up_next;
+                    sw_cell(H[c], hup, hl, el, sub, goe, ge, hn, en);
+                    if (c >= CPAD && gl == G - 1)
+                        hn = 0;
+                    H[c] = hn;
+                    hl = hn;
+                    el = en;
+                }
+                if (G > 1) {
+                    h_in = __shfl_up_sync(gmask, hl, 1, G);
+                    e_in = __shfl_up_sync(gmask, el, 1, G);
+                    if (gl == 0) {
+                        h_in = 0;
+                        e_in = 0;
+                    }
+                }
+                // first maximum of this row inside the matrix: key = H*256 + (255-c)
+                if (row_live) {
+                    int32_t rk = 0;
+                    if (ri0 + K - 1 < rlen) {
+#pragma unroll
+                        for (int c = 0; c < K; ++c)
+                            rk = max(rk, H[c] * 256 + (255 - c));
+                    } else {
+                        const int64_t lim = (int64_t)rlen - ri0;  // columns c < lim are inside
+#pragma unroll
+                        for (int c = 0; c < K; ++c)
+                            rk = max(rk, (c < lim) ? H[c] * 256 + (255 - c) : 0);
+                    }
+                    if ((rk >> 8) > best) {
+                        best = rk >> 8;
+                        bq = qi;
+                        bj = gl * K + 255 - (rk & 255);
+                    }
+                }
+            }
+            uint64_t key = 0;
+            if (best > 0)
+                key = ((uint64_t)best << 42) | ((uint64_t)(0x1FFFFF - bq) << 21) |
+                      (uint64_t)(0x1FFFFF - bj);
+#pragma unroll
+            for (int off = 1; off < G; off <<= 1) {
+                const uint64_t o = __shfl_xor_sync(gmask, key, off, G);
+                key = o > key ? o : key;
+            }
+            if (gl == 0)
+                sw_store(out, pi, key, B);
+        }
+        if (!queue_counter)
+            base += warps_total * PAIRS_PER_WARP;
+    }
+}
+
+// Literal per-pair kernel: one thread per pair, int64 arithmetic, rows in
+// global scratch.  Statement order follows align_cpu.mojo:239-309 exactly,
+// so it is exact for every configuration and band.
+__global__ void __launch_bounds__(128)
+sw_literal_kernel(SeqView q, SeqView r, SwParams p, int32_t band, const int32_t *__restrict__ bands,
+                  PairList pl, gb2_sw_result *__restrict__ out, int64_t *__restrict__ scratch,
+                  int64_t stride)
+{
+    int64_t n;
+    const int32_t *__restrict__ queue = pairs_resolve(pl, n);
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    int64_t *hp = scratch + tid * stride;
+    for (int64_t slot = tid; slot < n; slot += nth) {
+        const int64_t pi = queue ? (int64_t)queue[slot] : slot;
+        const int64_t b = bands ? bands[pi] : band;
+        const int64_t width = 2 * b + 1;
+        int64_t *hc = hp + width, *ec = hp + 2 * width;
+        const int64_t qlen = q.lengths[pi], rlen = r.lengths[pi];
+        const uint64_t *qw = q.packed + (q.offsets[pi] - q.word_base);
+        const uint64_t *rw = r.packed + (r.offsets[pi] - r.word_base);
+        int64_t best = 0, bq = 0, br = 0;
+        if (width > 0) {
+            for (int64_t j = 0; j < width; ++j)
+                hp[j] = 0;
+            for (int64_t qi = 0; qi < qlen; ++qi) {
+                for (int64_t j = 0; j < width; ++j) {
+                    hc[j] = 0;
+                    ec[j] = 0;
+                }
+                const int64_t qb = (int64_t)((qw[qi >> 5] >> (62 - 2 * (qi & 31))) & 3u);
+                for (int64_t off = 0; off < width; ++off) {
+                    const int64_t ri = qi - b + off;
+                    if (ri < 0 || ri >= rlen)
+                        continue;
+                    const int64_t rb = (int64_t)((rw[ri >> 5] >> (62 - 2 * (ri & 31))) & 3u);
+                    const int64_t sub = (qb == rb) ? p.match : p.mismatch;
+                    const int64_t h_diag = hp[off];
+                    const int64_t h_up = (off + 1 < width) ? hp[off + 1] : 0;
+                    const int64_t h_left = (off > 0) ? hc[off - 1] : 0;
+                    int64_t e1 = (off > 0) ? ec[off - 1] + p.ge : -1000000LL;
+                    int64_t e2 = h_up + p.go + p.ge;
+                    const int64_t e_val = e1 > e2 ? e1 : e2;
+                    const int64_t f_val = h_left + p.go + p.ge;
+                    int64_t cell = h_diag + sub;
+                    cell = cell > e_val ? cell : e_val;
+                    cell = cell > f_val ? cell : f_val;
+                    cell = cell > 0 ? cell : 0;
+                    hc[off] = cell;
+                    ec[off] = e_val;
+                    if (cell > best) {
+                        best = cell;
+                        bq = qi;
+                        br = ri;
+                    }
+                }
+                for (int64_t j = 0; j < width; ++j)
+                    hp[j] = hc[j];
+            }
+        }
+        gb2_sw_result res;
+        res.score = (int32_t)best;
+        res.query_end = (int32_t)bq;
+        res.ref_end = (int32_t)br;
+        out[pi] = res;
+    }
+}
+
+template <int B, int G, int K>
+static cudaError_t launch_band(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *out,
+                               int grid, cudaStream_t st)
+{
+    const int block = 128;
+    const int64_t pairs_per_block = (block / 32) * (32 / G);
+    int g = grid;
+    if (g <= 0) {  // one pass over a host-known count
+        if (pl.seg || pl.n <= 0)
+            return pl.n <= 0 && !pl.seg ? cudaSuccess : cudaErrorInvalidValue;
+        const int64_t need = (pl.n + pairs_per_block - 1) / pairs_per_block;
+        g = (int)(need < 0x7fffffff ? need : 0x7fffffff);
+    }
+    sw_band_kernel<B, G, K><<<g, block, 0, st>>>(q, r, p, pl, out);
+    return cudaGetLastError();
+}
+
+template <int B, int G, int K>
+static int occ_band()
+{
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sw_band_kernel<B, G, K>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+int sw_blocks_per_sm(int band_class, int variant)
+{
+    switch (band_class) {
+    case 16: return variant == 1 ? occ_band<16, 2, 17>() : occ_band<16, 1, 33>();
+    case 32:
+        return variant == 1 ? occ_band<32, 2, 33>()
+                            : (variant == 2 ? occ_band<32, 4, 17>() : occ_band<32, 1, 65>());
+    case 64: return variant == 1 ? occ_band<64, 4, 33>() : occ_band<64, 2, 65>();
+    case 128: return variant == 1 ? occ_band<128, 8, 33>() : occ_band<128, 4, 65>();
+    default: return 4;
+    }
+}
+
+int sw_pairs_per_block(int band_class, int variant)
+{
+    int G = 1;
+    switch (band_class) {
+    case 16: G = variant == 1 ? 2 : 1; break;
+    case 32: G = variant == 1 ? 2 : (variant == 2 ? 4 : 1); break;
+    case 64: G = variant == 1 ? 4 : 2; break;
+    case 128: G = variant == 1 ? 8 : 4; break;
+    default: return 128;
+    }
+    return 4 * (32 / G);
+}
+
+// variant selects (G, K) for a band class: 0 = default.
+cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParams p, int32_t band,
+                      const int32_t *bands, PairList pl, gb2_sw_result *out, int64_t *scratch,
+                      int64_t scratch_stride, int grid, cudaStream_t st)
+{
+    switch (band_class) {
+    case 16:
+        if (variant == 1)
+            return launch_band<16, 2, 17>(q, r, p, pl, out, grid, st);
+        return launch_band<16, 1, 33>(q, r, p, pl, out, grid, st);
+    case 32:
+        if (variant == 1)
+            return launch_band<32, 2, 33>(q, r, p, pl, out, grid, st);
+        if (variant == 2)
+            return launch_band<32, 4, 17>(q, r, p, pl, out, grid, st);
+        return launch_band<32, 1, 65>(q, r, p, pl, out, grid, st);
+    case 64:
+        if (variant == 1)
+            return launch_band<64, 4, 33>(q, r, p, pl, out, grid, st);
+        return launch_band<64, 2, 65>(q, r, p, pl, out, grid, st);
+    case 128:
+        if (variant == 1)
+            return launch_band<128, 8, 33>(q, r, p, pl, out, grid, st);
+        return launch_band<128, 4, 65>(q, r, p, pl, out, grid, st);
+    default: {
+        if (grid <= 0)
+            return cudaErrorInvalidValue;  // the literal kernel needs a sized scratch grid
+        sw_literal_kernel<<<grid, 128, 0, st>>>(q, r, p, band, bands, pl, out, scratch,
+                                                scratch_stride);
+        return cudaGetLastError();
+    }
+    }
+}
+
+}  // namespace gb2

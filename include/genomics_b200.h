@@ -1,0 +1,191 @@
+/*
+ * genomics_b200.h -- C ABI of libgenomics_b200.so, the B200 (sm_100a)
+ * batched pairwise-alignment library.
+ *
+ * The library computes exactly what the reference's CPU path computes:
+ *   - banded Smith-Waterman, genomics/cpu/align_cpu.mojo:229-309
+ *     (smith_waterman_banded): score, query_end, ref_end (starts are 0 and
+ *     the CIGAR is empty, align_cpu.mojo:302-309);
+ *   - gap-affine WFA cost, genomics/cpu/align_cpu.mojo:75-226
+ *     (wfa_affine_cpu): minimum cost or -1 past max_error;
+ * over sequences stored as the reference's SequenceBatch
+ * (genomics/core/sequence.mojo:23-36): 2-bit MSB-first packed uint64 words,
+ * one NMask word per packed word, per-sequence word offsets and lengths.
+ * N bases are stored as A (sequence.mojo:53-57) and compare equal to A.
+ *
+ * Conventions: every entry point returns an int status (GB2_OK == 0, the
+ * others negative; gb2_strerror names them).  The caller owns every host
+ * array; the library never keeps a host pointer after a call returns.
+ * Device batches belong to the context that made them.  Calls on one
+ * context are serialised by the context; separate contexts may be used
+ * from separate threads.
+ */
+#ifndef GENOMICS_B200_H
+#define GENOMICS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define GB2_OK 0
+#define GB2_EINVAL (-1)      /* bad argument (NULL, negative size, bad config) */
+#define GB2_ENOMEM (-2)      /* device or pinned allocation failed / over budget */
+#define GB2_ECUDA (-3)       /* a CUDA runtime call failed */
+#define GB2_ENODEV (-4)      /* no CUDA device, or not an sm_100 device */
+#define GB2_ERANGE (-5)      /* input outside the exact integer range */
+#define GB2_ETIMEOUT (-6)    /* a bounded wait ran out */
+#define GB2_ESTATE (-7)      /* wrong state (server not running, ...) */
+#define GB2_EKERNEL (-8)     /* a kernel reported an internal error flag */
+
+/* ---- configuration and result structs ------------------------------------- */
+
+/* AlignConfig (align_cpu.mojo:18-25).  Penalties are negative. */
+typedef struct {
+    int32_t match_score;
+    int32_t mismatch;
+    int32_t gap_open;
+    int32_t gap_extend;
+    int32_t band_width;
+} gb2_sw_cfg;
+
+/* AlignResult (align_cpu.mojo:28-36) minus the fields that are always zero
+   (query_start, ref_start) and the always-empty cigar. */
+typedef struct {
+    int32_t score;
+    int32_t query_end;
+    int32_t ref_end;
+} gb2_sw_result;
+
+/* WFAConfig (align_cpu.mojo:62-68).  Positive costs. */
+typedef struct {
+    int32_t x;
+    int32_t o;
+    int32_t e;
+    int32_t max_error;
+} gb2_wfa_cfg;
+
+typedef struct gb2_ctx gb2_ctx;
+typedef struct gb2_batch gb2_batch;
+
+/* ---- flags ------------------------------------------------------------------ */
+#define GB2_FLAG_PLAIN 0x0     /* one launch per band class, pairs in input order */
+#define GB2_FLAG_BATCHED 0x1   /* length-bucketed device work queue, persistent kernel */
+#define GB2_FLAG_INT32 0x2     /* never take the packed int16 Smith-Waterman path */
+#define GB2_FLAG_GENERIC 0x4   /* force the literal per-pair kernel (testing) */
+
+/* ---- library ----------------------------------------------------------------- */
+
+/* Library version as 10000*major + 100*minor + patch. */
+int gb2_version(void);
+
+/* Static string naming a status code. */
+const char *gb2_strerror(int status);
+
+/* ---- context (replaces GenomicsDevice, genomics/gpu/device.mojo:21-32) ------- */
+
+/* Create a context on CUDA device `device`: one stream set, pinned staging,
+   device scratch.  Fails with GB2_ENODEV when the device is not sm_100. */
+int gb2_create(int device, gb2_ctx **out);
+int gb2_destroy(gb2_ctx *ctx);
+
+/* Wait for all work queued on the context. */
+int gb2_sync(gb2_ctx *ctx);
+
+/* Last error text recorded on the context (for messages beyond the code). */
+const char *gb2_last_error(gb2_ctx *ctx);
+
+/* ---- device-resident SequenceBatch -------------------------------------------
+ * Replaces GenomicsDevice.upload_batch_packed / upload_lengths /
+ * upload_offsets (genomics/gpu/device.mojo:60-108): one pinned staging pass
+ * and asynchronous copies of the packed words, the NMask words (may be NULL:
+ * alignment never reads them), the word offsets and the lengths.  The
+ * batch stays on the device until gb2_batch_free. */
+int gb2_batch_upload(gb2_ctx *ctx, const uint64_t *packed, int64_t n_words,
+                     const uint64_t *nmask, const int64_t *offsets,
+                     const int64_t *lengths, int64_t count, gb2_batch **out);
+int gb2_batch_free(gb2_ctx *ctx, gb2_batch *batch);
+/* Number of sequences / packed words held by a batch. */
+int gb2_batch_info(const gb2_batch *batch, int64_t *count, int64_t *n_words);
+
+/* ---- batched banded Smith-Waterman --------------------------------------------
+ * Pair i = (query i of q, reference i of r), as launch_banded_sw
+ * (genomics/gpu/align_gpu.mojo:460-492).  `bands` (host, may be NULL) gives
+ * a per-pair band width that overrides cfg->band_width; `out` is a host
+ * array of n_pairs results.  Blocking. */
+int gb2_sw_banded(gb2_ctx *ctx, const gb2_batch *q, const gb2_batch *r,
+                  const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n_pairs,
+                  gb2_sw_result *out, int flags);
+
+/* Same, end to end from host SequenceBatch arrays: pinned staging, chunked
+   host-to-device copies overlapped with the kernels, results copied back.
+   Blocking. */
+int gb2_sw_banded_host(gb2_ctx *ctx,
+                       const uint64_t *q_packed, const int64_t *q_offsets,
+                       const int64_t *q_lengths,
+                       const uint64_t *r_packed, const int64_t *r_offsets,
+                       const int64_t *r_lengths,
+                       const gb2_sw_cfg *cfg, const int32_t *bands,
+                       int64_t n_pairs, gb2_sw_result *out, int flags);
+
+/* Per-pair drop-in for smith_waterman_banded(query, reference, cfg)
+   (align_cpu.mojo:229-233): raw word pointers of one SequenceView each
+   (sequence.mojo:78-94).  Upload, launch and synchronise on every call. */
+int gb2_sw_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
+                const uint64_t *r_words, int64_t rlen, const gb2_sw_cfg *cfg,
+                gb2_sw_result *out);
+
+/* ---- batched gap-affine WFA ----------------------------------------------------
+ * Pair i as above, as launch_wfa_affine (genomics/gpu/align_gpu.mojo:496-535)
+ * but with runtime penalties; out_cost is a host array (-1 = over
+ * max_error).  Requires x >= 1, e >= 1, o >= 0, max_error >= 0. */
+int gb2_wfa_affine(gb2_ctx *ctx, const gb2_batch *q, const gb2_batch *r,
+                   const gb2_wfa_cfg *cfg, int64_t n_pairs, int32_t *out_cost,
+                   int flags);
+
+int gb2_wfa_affine_host(gb2_ctx *ctx,
+                        const uint64_t *q_packed, const int64_t *q_offsets,
+                        const int64_t *q_lengths,
+                        const uint64_t *r_packed, const int64_t *r_offsets,
+                        const int64_t *r_lengths,
+                        const gb2_wfa_cfg *cfg, int64_t n_pairs,
+                        int32_t *out_cost, int flags);
+
+/* Per-pair drop-in for wfa_affine_cpu(query, ref_seq, cfg)
+   (align_cpu.mojo:75-79). */
+int gb2_wfa_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
+                 const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
+                 int32_t *out_cost);
+
+/* ---- pinned host memory -----------------------------------------------------------
+ * Page-locked host allocations: SequenceBatch arrays built here reach the
+ * device by DMA without the library's staging copy. */
+int gb2_host_alloc(int64_t bytes, void **out);
+int gb2_host_free(void *p);
+
+/* ---- measurement ------------------------------------------------------------------
+ * CUDA events recorded on the stream the alignment kernels run on. */
+int gb2_timer_start(gb2_ctx *ctx);
+int gb2_timer_stop(gb2_ctx *ctx, float *ms);
+/* Accumulated device time (ms) and launch count of the library's own
+   kernels since the last reset; kernel_ms covers the dominant kernels. */
+int gb2_stats(gb2_ctx *ctx, double *kernel_ms, int64_t *launches,
+              int64_t *work_units);
+int gb2_stats_reset(gb2_ctx *ctx);
+/* Enable per-launch event timing (adds two events per launch). */
+int gb2_set_profiling(gb2_ctx *ctx, int enable);
+/* Write `bytes` into a device buffer larger than L2 on the context stream
+   (L2 flush between timed iterations). */
+int gb2_flush_l2(gb2_ctx *ctx);
+/* Integer ALU throughput probe: runs dependent-chain microkernels of the
+   named instruction class over all SMs and reports giga-ops/s.  kind: 0 IADD,
+   1 IMNMX, 2 DPX viaddmax_s32, 3 DPX viaddmax_s16x2, 4 DPX vimax3_s32,
+   5 LOP3, 6 IMAD, 7 SHFL. */
+int gb2_int_peak(gb2_ctx *ctx, int kind, double *gops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GENOMICS_B200_H */

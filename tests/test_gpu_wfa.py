@@ -1,0 +1,113 @@
+"""Gap-affine WFA on the GPU against the oracle: bit-exact costs (-1 past
+max_error), through the C ABI."""
+import random
+
+import numpy as np
+import pytest
+
+import genomics_b200 as G
+from genomics_b200 import SequenceBatch, WFAConfig, synth
+from genomics_b200._lib import GenomicsError
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_wfa(O, q, r, cfg, envelope=True):
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    out, _ = O.wfa_batch(qp, qo, ql, rp, ro, rl, cfg.x, cfg.o, cfg.e, cfg.max_error,
+                         envelope=envelope)
+    return out
+
+
+def assert_same(got, ref, what=""):
+    bad = np.nonzero(got != ref)[0]
+    assert bad.size == 0, f"{what}: {bad.size} mismatches, first {bad[:5]} got {got[bad[:5]]} want {ref[bad[:5]]}"
+
+
+def test_known_answers_dropin(device, known):
+    cfg = G.default_wfa_config()
+    for case in known["wfa"]:
+        qb = SequenceBatch.from_strings([case["q"]])
+        rb = SequenceBatch.from_strings([case["r"]])
+        assert G.wfa_affine_cpu(G.get_view(qb, 0), G.get_view(rb, 0), cfg) == case["cost"], case["src"]
+
+
+def _mutated_pairs(rng, n, maxlen):
+    qs, rs = [], []
+    for _ in range(n):
+        q = "".join(rng.choice("ACGT") for _ in range(rng.randint(0, maxlen)))
+        if rng.random() < 0.8:
+            r = list(q)
+            for _k in range(rng.randint(0, max(1, len(q) // 10))):
+                pos = rng.randint(0, max(len(r) - 1, 0))
+                op = rng.random()
+                if op < 0.6 and r:
+                    r[pos] = rng.choice("ACGT")
+                elif op < 0.8:
+                    r[pos:pos] = rng.choice("ACGT") * rng.randint(1, 4)
+                elif r:
+                    del r[pos:pos + rng.randint(1, 4)]
+            r = "".join(r)
+        else:
+            r = "".join(rng.choice("ACGT") for _ in range(rng.randint(0, maxlen)))
+        qs.append(q)
+        rs.append(r)
+    return SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+
+
+@pytest.mark.parametrize("pen", [(4, 6, 2), (2, 3, 1), (1, 0, 1), (6, 4, 2), (3, 5, 2), (5, 2, 3)])
+def test_random_pairs(device, oracle, pen):
+    rng = random.Random(sum(pen))
+    q, r = _mutated_pairs(rng, 400, 400)
+    for me in (0, 7, 60, 200, 4000):
+        cfg = WFAConfig(*pen, me)
+        ref = oracle_wfa(oracle, q, r, cfg)
+        for batched in (True, False):
+            assert_same(device.wfa_affine(q, r, cfg, batched=batched), ref, f"{pen} me={me}")
+
+
+def test_statement_for_statement_oracle_small(device, oracle):
+    rng = random.Random(3)
+    q, r = _mutated_pairs(rng, 200, 80)
+    cfg = WFAConfig(4, 6, 2, 200)
+    ref = oracle_wfa(oracle, q, r, cfg, envelope=False)
+    assert_same(device.wfa_affine(q, r, cfg), ref, "faithful oracle")
+
+
+def test_edges(device, oracle):
+    qs = ["", "", "A", "", "ACGT", "A" * 64, "A" * 65, "ACGT" * 40, "N" * 50, "A" * 33]
+    rs = ["", "ACGT", "", "A" * 100, "ACGT", "A" * 65, "A" * 64, "TGCA" * 40, "A" * 50, "C" * 33]
+    q, r = SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+    for me in (0, 1, 8, 200, 1000):
+        cfg = WFAConfig(4, 6, 2, me)
+        assert_same(device.wfa_affine(q, r, cfg), oracle_wfa(oracle, q, r, cfg), f"me={me}")
+
+
+def test_workload2_sample_exact_cover(device, oracle):
+    q, r, _, _ = synth.generate(2, 3000)
+    me = synth.wfa_max_error_cover(q, r, 4, 6, 2)
+    cfg = WFAConfig(4, 6, 2, me)
+    ref = oracle_wfa(oracle, q, r, cfg)
+    assert (ref >= 0).all()
+    got = device.wfa_affine(q, r, cfg, batched=True)
+    assert_same(got, ref, "workload 2")
+    dq, dr = device.upload_batch(q), device.upload_batch(r)
+    assert_same(device.wfa_affine(dq, dr, cfg, batched=False), ref, "workload 2 resident plain")
+
+
+def test_workload2_max_error_200(device, oracle):
+    q, r, _, _ = synth.generate(2, 2000, seed=12)
+    cfg = WFAConfig(4, 6, 2, 200)
+    ref = oracle_wfa(oracle, q, r, cfg)
+    assert (ref == -1).any() and (ref >= 0).any()
+    assert_same(device.wfa_affine(q, r, cfg), ref, "max_error 200")
+
+
+def test_errors(device):
+    q = SequenceBatch.from_strings(["ACGT"])
+    r = SequenceBatch.from_strings(["ACGT"])
+    for bad in (WFAConfig(0, 6, 2, 10), WFAConfig(4, 6, 0, 10), WFAConfig(4, -1, 2, 10),
+                WFAConfig(4, 6, 2, -1), WFAConfig(100, 6, 1, 10)):
+        with pytest.raises(GenomicsError):
+            device.wfa_affine(q, r, bad)

@@ -1,0 +1,175 @@
+"""The oracle pinned against the reference's own known answers, and against an
+independent small restatement.  CPU only."""
+import random
+
+import numpy as np
+import pytest
+
+# default_config (genomics/cpu/align_cpu.mojo:46-53)
+DEF = dict(match=2, mismatch=-3, gap_open=-5, gap_extend=-2)
+
+
+def test_sw_known_answers(oracle, known):
+    for case in known["sw"]:
+        s = oracle.sw_banded(case["q"], case["r"], band=case["band"], **DEF)
+        if "score" in case:
+            assert s[0] == case["score"], case["src"]
+        else:
+            assert s[0] >= case["score_at_least"] and s[0] > 0, case["src"]
+        assert s[1] == 0 and s[2] == 0
+
+
+def test_nw_known_answers(oracle, known):
+    for case in known["nw"]:
+        s = oracle.nw_banded(case["q"], case["r"], band=case["band"], **DEF)
+        assert s[0] == case["score"], case["src"]
+
+
+def test_wfa_known_answers(oracle, known):
+    for case in known["wfa"]:
+        assert oracle.wfa_affine(case["q"], case["r"]) == case["cost"], case["src"]
+        assert oracle.wfa_affine(case["q"], case["r"], envelope=True) == case["cost"], case["src"]
+
+
+def _cigar_cost(cigar, x, o, e):
+    """tests/test_alignment.mojo:145-166."""
+    cost, cnt = 0, 0
+    for ch in cigar:
+        if ch.isdigit():
+            cnt = cnt * 10 + int(ch)
+        else:
+            if ch == "X":
+                cost += cnt * x
+            elif ch in "ID":
+                cost += o + cnt * e
+            cnt = 0
+    return cost
+
+
+def _cigar_len(cigar, ops):
+    tot, cnt = 0, 0
+    for ch in cigar:
+        if ch.isdigit():
+            cnt = cnt * 10 + int(ch)
+        else:
+            if ch in ops:
+                tot += cnt
+            cnt = 0
+    return tot
+
+
+def test_wfa_cigar_known_answers(oracle, known):
+    for case in known["wfa_cigar"]:
+        cost, cig = oracle.wfa_cigar(case["q"], case["r"])
+        assert cost == case["cost"] and cig == case["cigar"], case["src"]
+    for q, r in known["wfa_cigar_consistency"]["pairs"]:
+        cost, cig = oracle.wfa_cigar(q, r)
+        assert cost == oracle.wfa_affine(q, r)
+        assert _cigar_cost(cig, 4, 6, 2) == cost
+        assert _cigar_len(cig, "=XI") == len(q)
+        assert _cigar_len(cig, "=XD") == len(r)
+
+
+def test_encoding_known_answers(oracle, known):
+    enc = known["encoding"]
+    for c, v in enc["ascii_to_2bit"]["cases"]:
+        assert oracle.lib().or_ascii_to_2bit(c) == v
+    w = np.array([int(enc["get_base_from_word"]["word_hex"], 16)], np.uint64)
+    for i, b in enumerate(enc["get_base_from_word"]["bases"]):
+        assert oracle.lib().or_get_base_export(oracle._p(w, oracle._u64p), i) == b
+    p, m = oracle.pack(enc["view_33"]["seq"])
+    assert p.size == enc["view_33"]["word_count"]
+    assert int(p[1] >> np.uint64(62)) == enc["view_33"]["last_base"]
+    p, m = oracle.pack(enc["n_tracking"]["seq"])
+    assert [bool((int(m[0]) >> i) & 1) for i in range(4)] == enc["n_tracking"]["is_n"]
+
+
+# ---- an independent, deliberately naive restatement for small cases ----------------
+
+def _base(s, i):
+    return {"A": 0, "C": 1, "G": 2, "T": 3}.get(s[i].upper(), 0)
+
+
+def _sw_naive(q, r, m, mm, go, ge, b):
+    """Band cell (qi, j), ri = qi - b + j; dictionaries default to 0 for
+    skipped cells, which is what align_cpu.mojo:261-263 resets them to."""
+    H, E = {}, {}
+    best = (0, 0, 0)
+    for qi in range(len(q)):
+        for j in range(2 * b + 1):
+            ri = qi - b + j
+            if ri < 0 or ri >= len(r):
+                continue
+            sub = m if _base(q, qi) == _base(r, ri) else mm
+            hd = H.get((qi - 1, j), 0)
+            hu = H.get((qi - 1, j + 1), 0) if j + 1 <= 2 * b else 0
+            hl = H.get((qi, j - 1), 0) if j > 0 else 0
+            el = E.get((qi, j - 1), 0) + ge if j > 0 else -1000000
+            e = max(el, hu + go + ge)
+            f = hl + go + ge
+            h = max(0, hd + sub, e, f)
+            H[(qi, j)] = h
+            E[(qi, j)] = e
+            if h > best[0]:
+                best = (h, qi, ri)
+    return best
+
+
+def _rand_seq(rng, n, alphabet="ACGT"):
+    return "".join(rng.choice(alphabet) for _ in range(n))
+
+
+def test_sw_matches_naive_restatement(oracle):
+    rng = random.Random(7)
+    for _ in range(300):
+        q = _rand_seq(rng, rng.randint(0, 40), "ACGTN")
+        r = _rand_seq(rng, rng.randint(0, 40), "ACGTN")
+        if rng.random() < 0.5 and q:
+            r = q[: rng.randint(0, len(q))] + _rand_seq(rng, rng.randint(0, 8))
+        b = rng.randint(0, 12)
+        prm = (rng.randint(0, 4), -rng.randint(0, 5), -rng.randint(0, 6), -rng.randint(0, 3))
+        if rng.random() < 0.1:  # configurations outside the usual signs
+            prm = (rng.randint(-2, 4), rng.randint(-5, 3), rng.randint(-6, 3), rng.randint(-3, 2))
+        got = oracle.sw_banded(q, r, *prm, band=b)
+        s, qi, ri = _sw_naive(q, r, *prm, b)
+        assert (got[0], got[3], got[4]) == (s, qi, ri), (q, r, prm, b)
+
+
+def test_wfa_envelope_equals_statement_for_statement(oracle):
+    rng = random.Random(11)
+    for _ in range(400):
+        q = _rand_seq(rng, rng.randint(0, 60))
+        if rng.random() < 0.7 and q:
+            r = list(q)
+            for _k in range(rng.randint(0, 8)):
+                op = rng.random()
+                pos = rng.randint(0, max(len(r) - 1, 0))
+                if op < 0.5 and r:
+                    r[pos] = rng.choice("ACGT")
+                elif op < 0.75:
+                    r.insert(pos, rng.choice("ACGT"))
+                elif r:
+                    del r[pos]
+            r = "".join(r)
+        else:
+            r = _rand_seq(rng, rng.randint(0, 60))
+        x, o, e = rng.randint(1, 6), rng.randint(0, 8), rng.randint(1, 4)
+        me = rng.choice([0, 1, 5, 20, 60, 200])
+        a = oracle.wfa_affine(q, r, x, o, e, me)
+        b = oracle.wfa_affine(q, r, x, o, e, me, envelope=True)
+        assert a == b, (q, r, x, o, e, me)
+
+
+def test_wfa_batch_driver_matches_single(oracle):
+    from genomics_b200 import synth
+    q, r, _, _ = synth.generate(2, 40, seed=5)
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    me = synth.wfa_max_error_cover(q, r, 4, 6, 2)
+    env, work = oracle.wfa_batch(qp, qo, ql, rp, ro, rl, 4, 6, 2, me, envelope=True, threads=4)
+    assert (env >= 0).all() and work[0] > 0
+    # the statement-for-statement routine on the shortest pairs
+    for i in np.argsort(ql)[:8]:
+        w = oracle.lib().or_wfa_affine(oracle._p(qp[qo[i]:], oracle._u64p), int(ql[i]),
+                                       oracle._p(rp[ro[i]:], oracle._u64p), int(rl[i]), 4, 6, 2, me)
+        assert w == env[i]
