@@ -14,7 +14,9 @@ around its origin, 2% substitutions + 0.5% indels, band 32, scores
               from pinned host arrays: host->device copies of the packed words,
               offsets and lengths and the device->host copy of the results are
               inside the timed region.
-  roofline    integer-ALU view of the dominant kernel.
+  roofline    integer-ALU view of the dominant kernel: cells x 11 int32 ops (the
+              reference recurrence as written) against the lane-op peak measured by
+              the library's own microkernels in the same run; an HBM view beside it.
   cpu_baseline  the C oracle (restatement of align_cpu.mojo) on a bounded
               sample of the same workload, all host threads.
 
