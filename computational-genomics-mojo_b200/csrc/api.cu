@@ -705,6 +705,7 @@ const char *gb2_strerror(int status)
     case GB2_ETIMEOUT: return "timed out";
     case GB2_ESTATE: return "wrong state";
     case GB2_EKERNEL: return "kernel reported an error";
+    case GB2_ESCRATCH: return "request exceeds the fixed no-allocation scratch";
     default: return "unknown status";
     }
 }

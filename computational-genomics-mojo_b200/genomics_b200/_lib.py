@@ -24,6 +24,7 @@ GB2_ERANGE = -5
 GB2_ETIMEOUT = -6
 GB2_ESTATE = -7
 GB2_EKERNEL = -8
+GB2_ESCRATCH = -9
 
 FLAG_PLAIN = 0x0
 FLAG_BATCHED = 0x1
@@ -65,6 +66,8 @@ SIGNATURES = [
     ("gb2_wfa_affine_host", ctypes.c_int,
      [vp, vp, vp, vp, vp, vp, vp, P(WfaCfg), c_i64, vp, ctypes.c_int]),
     ("gb2_wfa_pair", ctypes.c_int, [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32)]),
+    ("gb2_wfa_affine_noalloc", ctypes.c_int,
+     [vp, c_i64, vp, vp, vp, c_i64, vp, vp, c_i64, c_i64, P(WfaCfg), c_i64, vp, vp]),
     ("gb2_host_alloc", ctypes.c_int, [c_i64, P(vp)]),
     ("gb2_host_free", ctypes.c_int, [vp]),
     ("gb2_timer_start", ctypes.c_int, [vp]),

@@ -39,6 +39,7 @@ extern "C" {
 #define GB2_ETIMEOUT (-6)    /* a bounded wait ran out */
 #define GB2_ESTATE (-7)      /* wrong state (server not running, ...) */
 #define GB2_EKERNEL (-8)     /* a kernel reported an internal error flag */
+#define GB2_ESCRATCH (-9)    /* request too large for the fixed no-allocation scratch */
 
 /* ---- configuration and result structs ------------------------------------- */
 
@@ -158,6 +159,31 @@ int gb2_wfa_affine_host(gb2_ctx *ctx,
 int gb2_wfa_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
                  const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
                  int32_t *out_cost);
+
+/* ---- gap-affine WFA with no device allocation ------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code whose device memory belongs to a host runtime's own allocator,
+ * plug-ins held to a fixed memory budget, request loops that must not
+ * allocate.  Inputs and outputs are the caller's device pointers: per side a
+ * SequenceBatch (packed words, int64 offsets, int64 lengths) and n_pairs
+ * int32 costs out.  The wavefront scratch is a fixed device array of
+ * GB2_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
+ * it until the process exits.  max_qlen / max_rlen bound the lengths: a
+ * request whose rings ((max(x,o+e)/g + 1 + 2(e/g + 1)) slots x
+ * (max_qlen + max_rlen + 5) int32 per warp, g = gcd(x, o, e)) leave room for
+ * fewer than four warps returns GB2_ESCRATCH; a pair longer than stated gets
+ * cost -2 and the call returns GB2_EINVAL.  Blocking on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  The first call on a
+ * device looks up the array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+#define GB2_NOALLOC_SCRATCH_BYTES (32ll << 20)
+int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
+                           const int64_t *q_offsets, const int64_t *q_lengths,
+                           const uint64_t *r_packed, int64_t r_words,
+                           const int64_t *r_offsets, const int64_t *r_lengths,
+                           int64_t max_qlen, int64_t max_rlen,
+                           const gb2_wfa_cfg *cfg, int64_t n_pairs,
+                           int32_t *out_cost, void *stream);
 
 /* ---- pinned host memory -----------------------------------------------------------
  * Page-locked host allocations: SequenceBatch arrays built here reach the
