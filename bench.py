@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--no-peaks", action="store_true", help="skip the integer-throughput probes")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant knob (tuning)")
     ap.add_argument("--plain", action="store_true", help="plain launch instead of the queue")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-band SW, long-pair WFA and per-call measurements")
+    ap.add_argument("--extras-only", action="store_true", help="(tuning) only the extras")
     return ap.parse_args()
 
 
@@ -340,10 +343,188 @@ def our_arm(args, dist: Dist):
         }
     dq.close()
     dr.close()
+    if line is not None and dist.world == 1 and not args.no_extras:
+        line["extras"] = extras(args, dev)
     dev.close()
     dist.close()
     if line:
         print(json.dumps(line), flush=True)
+
+
+def _time_steps(dev, fn, steps, warmup):
+    """Device time (ms) per step of fn() on the library stream, L2 flushed between."""
+    for _ in range(warmup):
+        dev.flush_l2()
+        fn()
+    ts = []
+    for _ in range(steps):
+        dev.flush_l2()
+        dev.timer_start()
+        fn()
+        ts.append(dev.timer_stop())
+    return statistics.median(ts)
+
+
+def extras(args, dev):
+    """Batched queue vs plain launch vs per-call drop-in on the mixed-length workloads,
+    with the CPU restatement of the reference beside each (all host threads)."""
+    import oracle as O
+    from genomics_b200 import AlignConfig, WFAConfig, synth
+    O.build()
+    threads = os.cpu_count() or 1
+    out = {}
+    # mixed-band SW: 200,000 pairs, 100-2,000 bp, bands {16,32,64,128}, N runs
+    q, r, bands, _ = synth.generate(3, 200_000)
+    cfg = AlignConfig(*SCORING, 32)
+    cells = synth.sw_cells(q, bands)
+    dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
+    tb = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=True), 3, 2)
+    tp = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=False), 3, 2)
+    m = 3000
+    t0 = time.perf_counter()
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    for i in range(m):
+        c_i = AlignConfig(*SCORING, int(bands[i]))
+        dev.sw_pair(qp[qo[i]:qo[i] + (ql[i] + 31) // 32], int(ql[i]),
+                    rp[ro[i]:ro[i] + (rl[i] + 31) // 32], int(rl[i]), c_i)
+    tcall = time.perf_counter() - t0
+    call_cells = int((ql[:m] * (2 * bands[:m].astype(np.int64) + 1)).sum())
+    ns = 20_000
+    t0 = time.perf_counter()
+    O.sw_batch(qp, qo[:ns], ql[:ns], rp, ro[:ns], rl[:ns], *SCORING, 32, bands=bands[:ns],
+               threads=threads)
+    tcpu = time.perf_counter() - t0
+    cpu_cells = int((ql[:ns] * (2 * bands[:ns].astype(np.int64) + 1)).sum())
+    out["mixed_sw_200k"] = {
+        "workload": "200,000 pairs, query 100-2,000 bp, target 1.25x, bands {16,32,64,128}, "
+                    "1-8% divergence, 1% N runs, +2/-4/-4/-2",
+        "cells": cells,
+        "batched_gcups": round(cells / tb / 1e6, 2), "batched_ms": round(tb, 3),
+        "plain_launch_gcups": round(cells / tp / 1e6, 2), "plain_launch_ms": round(tp, 3),
+        "per_call_gcups": round(call_cells / tcall / 1e9, 3),
+        "per_call_pairs_per_s": round(m / tcall, 1),
+        "batched_over_per_call": round((cells / tb / 1e6) / (call_cells / tcall / 1e9), 1),
+        "cpu_gcups": round(cpu_cells / tcpu / 1e9, 3), "cpu_cores": threads,
+        "cpu_sample": f"first {ns} pairs",
+    }
+    dq.close()
+    dr.close()
+    # long WFA: 100,000 pairs, 100-10,000 bp, 1-10% divergence, x4 o6 e2
+    q, r, _, _ = synth.generate(2, 100_000)
+    me = synth.wfa_max_error_cover(q, r, 4, 6, 2)
+    wcfg = WFAConfig(4, 6, 2, me)
+    dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
+    n = 100_000
+    dev.stats_reset()
+    tb = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True), 2, 1)
+    wcells = dev.stats()["work_units"] // 3
+    tp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False), 2, 1)
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    m = 300
+    t0 = time.perf_counter()
+    for i in range(m):
+        dev.wfa_pair(qp[qo[i]:qo[i] + (ql[i] + 31) // 32], int(ql[i]),
+                     rp[ro[i]:ro[i] + (rl[i] + 31) // 32], int(rl[i]), wcfg)
+    tcall = time.perf_counter() - t0
+    ns = 96
+    t0 = time.perf_counter()
+    O.wfa_batch(qp, qo[:ns], ql[:ns], rp, ro[:ns], rl[:ns], 4, 6, 2, me, envelope=False,
+                threads=threads)
+    tcpu = time.perf_counter() - t0
+    out["wfa_100k"] = {
+        "workload": "100,000 pairs, 100-10,000 bp log-uniform, 1-10% divergence (70% subst., "
+                    "30% indels), x4 o6 e2",
+        "max_error": me, "max_error_rule": "largest per-pair exact-cover bound (no pair -1)",
+        "wavefront_cells": int(wcells),
+        "batched_pairs_per_s": round(n / (tb * 1e-3), 1), "batched_ms": round(tb, 3),
+        "plain_launch_pairs_per_s": round(n / (tp * 1e-3), 1), "plain_launch_ms": round(tp, 3),
+        "per_call_pairs_per_s": round(m / tcall, 1),
+        "batched_over_per_call": round((n / (tb * 1e-3)) / (m / tcall), 1),
+        "cpu_pairs_per_s": round(ns / tcpu, 2), "cpu_cores": threads,
+        "cpu_sample": f"first {ns} pairs, statement-for-statement port (per-score reset of "
+                      f"2*max_error+1 diagonals, as the reference)",
+    }
+    dq.close()
+    dr.close()
+    out["serving"] = serve_bench(dev)
+    return out
+
+
+def _slice(batch, i0, i1):
+    """Pairs [i0, i1) of an append-layout SequenceBatch, without copying words."""
+    from genomics_b200 import SequenceBatch
+    p, m, o, l = batch.arrays()
+    w0 = int(o[i0])
+    w1 = int(o[i1 - 1] + (l[i1 - 1] + 31) // 32)
+    return SequenceBatch.from_arrays(p[w0:w1], m[w0:w1], o[i0:i1] - w0, l[i0:i1])
+
+
+def serve_bench(dev, seconds_per_level=4.0, pool_pairs=40_000):
+    """Served mixed stream: Poisson arrivals of requests of 1-4,096 pairs (log-uniform),
+    each pair SW (band 32/64/128) or WFA, 100-20,000 bp, divergence up to 15%.
+    The peak is the completion rate with the queue kept full; each load level then
+    offers f x peak requests/s for a few seconds.  Latency = submit to results written,
+    measured by the server."""
+    import threading
+    from genomics_b200 import AlignConfig, WFAConfig, synth
+    from genomics_b200.serve import AlignmentServer
+    q, r, bands, kinds = synth.generate(4, pool_pairs)
+    swc = AlignConfig(*SCORING, 32)
+    wcfg = WFAConfig(4, 6, 2, synth.wfa_max_error_cover(q, r, 4, 6, 2))
+    rng = np.random.default_rng(0xB2000004)
+    n_req = 4096
+    sizes = np.minimum(np.round(np.exp(rng.uniform(0, np.log(4096), n_req))).astype(int), 4096)
+    starts = rng.integers(0, pool_pairs - 4096, n_req)
+
+    def make(j):
+        i0, i1 = int(starts[j]), int(starts[j] + sizes[j])
+        return (_slice(q, i0, i1), _slice(r, i0, i1), bands[i0:i1], kinds[i0:i1])
+
+    res = {"workload": "requests of 1-4,096 pairs (log-uniform), each pair SW (band 32/64/128) "
+                       "or WFA (p=0.5), 100-20,000 bp log-uniform, divergence 0-15%",
+           "max_error": int(wcfg.max_error)}
+    with AlignmentServer(dev, hbm_budget_bytes=32 << 30, max_inflight_groups=4) as srv:
+        # peak: 64 requests submitted at once
+        reqs = [make(j) for j in range(64)]
+        t0 = time.perf_counter()
+        prs = [srv.submit(a, b, swc, wcfg, kinds=k, bands=bd) for a, b, bd, k in reqs]
+        for pr in prs:
+            pr.wait(600_000)
+        t_peak = time.perf_counter() - t0
+        peak = len(prs) / t_peak
+        pairs = int(sum(len(x[2]) for x in reqs))
+        res["peak_requests_per_s"] = round(peak, 2)
+        res["peak_pairs_per_s"] = round(pairs / t_peak, 1)
+        levels = []
+        jbase = 64
+        for f in (0.2, 0.4, 0.6, 0.8, 1.0):
+            lam = f * peak
+            n_lvl = max(8, int(lam * seconds_per_level))
+            arrivals = np.cumsum(rng.exponential(1.0 / lam, n_lvl))
+            batch = [make((jbase + j) % n_req) for j in range(n_lvl)]
+            jbase += n_lvl
+            prs = []
+            tstart = time.perf_counter()
+            for j, (a, b, bd, k) in enumerate(batch):
+                delay = tstart + arrivals[j] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                prs.append(srv.submit(a, b, swc, wcfg, kinds=k, bands=bd))
+            for pr in prs:
+                pr.wait(600_000)
+            t_all = time.perf_counter() - tstart
+            lat = np.array([pr.latency_ms for pr in prs])
+            levels.append({"offered_fraction": f, "offered_requests_per_s": round(lam, 2),
+                           "requests": n_lvl,
+                           "pairs_per_s": round(sum(len(x[2]) for x in batch) / t_all, 1),
+                           "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                           "p99_ms": round(float(np.percentile(lat, 99)), 2)})
+        res["levels"] = levels
+        res["p99_ms_at_0.8"] = next(l["p99_ms"] for l in levels if l["offered_fraction"] == 0.8)
+        res["server"] = srv.stats()
+    return res
 
 
 def main():

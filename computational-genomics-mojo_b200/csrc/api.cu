@@ -1,83 +1,33 @@
 // api.cu -- the C ABI of libgenomics_b200.so (include/genomics_b200.h).
 //
-// Host runtime around the kernels: contexts (one compute stream, one copy
-// stream, auxiliary streams for concurrent band classes), device-resident
+// Host runtime around the kernels: contexts and executors (a stream plus
+// the planning and scratch buffers its launches use), device-resident
 // SequenceBatches uploaded through pinned staging, device-side length
 // bucketing of pair lists, the chunked host-to-device pipeline of the
 // end-to-end entry points, and the per-pair drop-in calls.
 #include <algorithm>
-#include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
-#include <string>
-#include <vector>
+#include <thread>
 
-#include "gb2_internal.cuh"
+#include "runtime.cuh"
 
 using namespace gb2;
 
 #define GB2_VERSION_NUM 100  // 0.1.0
-
-struct gb2_batch {
-    uint64_t *d_packed = nullptr;
-    uint64_t *d_nmask = nullptr;
-    int64_t *d_offsets = nullptr;
-    int64_t *d_lengths = nullptr;
-    int64_t count = 0, n_words = 0, max_len = 0;
-    gb2_ctx *owner = nullptr;
-};
+#define CU GB2_CU
 
 namespace {
-
-constexpr int kAux = 4;            // auxiliary streams for concurrent band classes
-constexpr int kSwClasses = 5;      // 16, 32, 64, 128, literal
-constexpr int kLenBuckets = 1024;  // length buckets per class
-constexpr int64_t kPinChunk = 32ll << 20;
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-};
-
-// One set of device buffers of the end-to-end pipeline.
-struct PipeSet {
-    DevBuf qw, rw, qo, ql, ro, rl, bands, out;
-    cudaEvent_t copied = nullptr, done = nullptr;
-};
-
+constexpr size_t kCounterBytes = 4096;  // dynamic-queue counters, 128 B apart
+constexpr int kCounterStride = 32;      // ints between the counters of two classes
 }  // namespace
 
-struct gb2_ctx {
-    int device = 0;
-    int sm_count = 148;
-    cudaStream_t st = nullptr, st_copy = nullptr;
-    cudaStream_t aux[kAux] = {};
-    cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
-    std::mutex mu;
-    std::string last_error;
-    // planning buffers
-    DevBuf keys, queue, counts, seg, counters, out_sw, out_wfa, bands, scratch64, scratch32,
-        work, errflag, flush, one_pair;
-    // pinned staging (two halves for double buffering)
-    void *pin[2] = {nullptr, nullptr};
-    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
-    void *pin_out = nullptr;
-    size_t pin_out_cap = 0;
-    PipeSet pipe[2];
-    // stats
-    bool profiling = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pending;
-    double kernel_ms = 0.0;
-    int64_t launches = 0;
-    int64_t work_units = 0;
-};
+namespace gb2 {
 
 // ---------------------------------------------------------------------------
-// error plumbing
+// plumbing
 // ---------------------------------------------------------------------------
-static int set_err(gb2_ctx *c, int code, const char *fmt, ...)
+int set_err(gb2_ctx *c, int code, const char *fmt, ...)
 {
     if (c) {
         char buf[512];
@@ -85,26 +35,61 @@ static int set_err(gb2_ctx *c, int code, const char *fmt, ...)
         va_start(ap, fmt);
         vsnprintf(buf, sizeof buf, fmt, ap);
         va_end(ap);
+        std::lock_guard<std::mutex> lk(c->err_mu);
         c->last_error = buf;
     }
     return code;
 }
 
-#define CU(ctx, call)                                                                    \
-    do {                                                                                 \
-        cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
-            return set_err((ctx), e_ == cudaErrorMemoryAllocation ? GB2_ENOMEM : GB2_ECUDA, \
-                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,    \
-                           __LINE__);                                                    \
-    } while (0)
+int exec_init(Exec &x)
+{
+    bool ok = cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&x.ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < kAux; ++i)
+        ok = cudaStreamCreateWithFlags(&x.aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&x.ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok)
+        cudaGetLastError();
+    return ok ? GB2_OK : GB2_ECUDA;
+}
 
-static int ensure(gb2_ctx *c, DevBuf &b, size_t bytes)
+void exec_free(Exec &x)
+{
+    if (x.st)
+        cudaStreamSynchronize(x.st);
+    for (int i = 0; i < kAux; ++i)
+        if (x.aux[i])
+            cudaStreamSynchronize(x.aux[i]);
+    DevBuf *bufs[] = {&x.keys,      &x.queue,     &x.counts, &x.seg,  &x.counters,
+                      &x.scratch64, &x.scratch32, &x.work,   &x.errflag};
+    for (DevBuf *b : bufs)
+        if (b->p) {
+            cudaFree(b->p);
+            b->p = nullptr;
+            b->cap = 0;
+        }
+    for (int i = 0; i < kAux; ++i) {
+        if (x.aux[i])
+            cudaStreamDestroy(x.aux[i]);
+        if (x.ev_join[i])
+            cudaEventDestroy(x.ev_join[i]);
+        x.aux[i] = nullptr;
+        x.ev_join[i] = nullptr;
+    }
+    if (x.ev_fork)
+        cudaEventDestroy(x.ev_fork);
+    if (x.st)
+        cudaStreamDestroy(x.st);
+    x.ev_fork = nullptr;
+    x.st = nullptr;
+}
+
+int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st)
 {
     if (bytes <= b.cap)
         return GB2_OK;
     if (b.p) {
-        CU(c, cudaStreamSynchronize(c->st));
+        CU(c, cudaStreamSynchronize(st));
         cudaFree(b.p);
         b.p = nullptr;
         b.cap = 0;
@@ -116,7 +101,7 @@ static int ensure(gb2_ctx *c, DevBuf &b, size_t bytes)
     return GB2_OK;
 }
 
-static bool is_pinned(const void *p)
+bool is_pinned(const void *p)
 {
     if (!p)
         return false;
@@ -128,10 +113,7 @@ static bool is_pinned(const void *p)
     return a.type == cudaMemoryTypeHost;
 }
 
-// Host-to-device copy on `st`.  Pinned sources go straight to the DMA
-// engine; pageable sources pass through the two pinned staging halves, the
-// host memcpy of one half overlapping the DMA of the other.
-static int h2d(gb2_ctx *c, void *dst, const void *src, size_t bytes, cudaStream_t st)
+int h2d(gb2_ctx *c, void *dst, const void *src, size_t bytes, cudaStream_t st)
 {
     if (bytes == 0)
         return GB2_OK;
@@ -139,10 +121,11 @@ static int h2d(gb2_ctx *c, void *dst, const void *src, size_t bytes, cudaStream_
         CU(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
         return GB2_OK;
     }
+    std::lock_guard<std::mutex> lk(c->pin_mu);
     size_t done = 0;
     int half = 0;
     while (done < bytes) {
-        size_t n = std::min<size_t>(bytes - done, (size_t)kPinChunk);
+        const size_t n = std::min<size_t>(bytes - done, (size_t)kPinChunk);
         CU(c, cudaEventSynchronize(c->pin_ev[half]));
         memcpy(c->pin[half], (const char *)src + done, n);
         CU(c, cudaMemcpyAsync((char *)dst + done, c->pin[half], n, cudaMemcpyHostToDevice, st));
@@ -153,11 +136,15 @@ static int h2d(gb2_ctx *c, void *dst, const void *src, size_t bytes, cudaStream_
     return GB2_OK;
 }
 
-static void harvest_profile(gb2_ctx *c)
+int64_t words_for(int64_t len) { return (len + 31) / 32; }
+
+void harvest_profile(gb2_ctx *c)
 {
+    std::lock_guard<std::mutex> lk(c->prof_mu);
     for (auto &pr : c->prof_pending) {
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess)
+        if (cudaEventSynchronize(pr.second) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess)
             c->kernel_ms += ms;
         else
             cudaGetLastError();
@@ -167,9 +154,11 @@ static void harvest_profile(gb2_ctx *c)
     c->prof_pending.clear();
 }
 
+}  // namespace gb2
+
 static cudaEvent_t prof_begin(gb2_ctx *c, cudaStream_t st)
 {
-    if (!c->profiling)
+    if (!c->profiling.load())
         return nullptr;
     cudaEvent_t a;
     cudaEventCreate(&a);
@@ -184,6 +173,7 @@ static void prof_end(gb2_ctx *c, cudaEvent_t a, cudaStream_t st)
     cudaEvent_t b;
     cudaEventCreate(&b);
     cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> lk(c->prof_mu);
     c->prof_pending.emplace_back(a, b);
 }
 
@@ -191,14 +181,25 @@ static void prof_end(gb2_ctx *c, cudaEvent_t a, cudaStream_t st)
 // device-side bucketing: pairs -> queue ordered by class, then by length
 // (longest first), with per-class [start, end) segments
 // ---------------------------------------------------------------------------
-__global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *bands, int32_t band,
-                              int fast_ok, int32_t match_pos, int32_t *keys, int *counts)
+// One atomic per distinct key in the warp (lanes with equal keys aggregate):
+// a uniform batch would otherwise serialise every pair on one counter.
+__device__ __forceinline__ void count_key(int *counts, int key)
 {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned mask = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == __ffs(mask) - 1)
+        atomicAdd(&counts[key], __popc(mask));
+}
+
+__global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *bands, int32_t band,
+                              int fast_ok, int pack_ok, int32_t match_pos, int32_t *keys,
+                              int *counts)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const int64_t ql = q.lengths[i], rl = r.lengths[i];
     const int32_t b = bands ? bands[i] : band;
+    const int64_t hmax = (int64_t)match_pos * (ql < rl ? ql : rl);  // bound on every H
     int cls = 4;
     if (fast_ok) {
         if (b == 16)
@@ -210,28 +211,30 @@ __global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *ba
         else if (b == 128)
             cls = 3;
     }
-    if (ql >= (1 << 21) - 1 || (int64_t)match_pos * (ql < rl ? ql : rl) >= (1ll << 22))
+    if (ql >= (1 << 21) - 1 || hmax >= (1ll << 22))
         cls = 4;
+    if (pack_ok && hmax <= kPackHmax && (cls == 0 || cls == 1))
+        cls = cls == 0 ? 5 : 6;
     int64_t lb = ql >> 5;
     if (lb > kLenBuckets - 1)
         lb = kLenBuckets - 1;
     const int key = cls * kLenBuckets + (kLenBuckets - 1 - (int)lb);
     keys[i] = key;
-    atomicAdd(&counts[key], 1);
+    count_key(counts, key);
 }
 
 __global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int32_t *keys, int *counts)
 {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    int64_t l = q.lengths[i] > r.lengths[i] ? q.lengths[i] : r.lengths[i];
+    const int64_t l = q.lengths[i] > r.lengths[i] ? q.lengths[i] : r.lengths[i];
     int64_t lb = l >> 4;
     if (lb > kLenBuckets - 1)
         lb = kLenBuckets - 1;
     const int key = kLenBuckets - 1 - (int)lb;
     keys[i] = key;
-    atomicAdd(&counts[key], 1);
+    count_key(counts, key);
 }
 
 // Exclusive scan of counts[nb] (one block); writes cursors into counts and
@@ -249,7 +252,7 @@ __global__ void k_scan(int *counts, int nb, int per_class, int64_t *seg)
     if (t == 0) {
         int acc = 0;
         for (int i = 0; i < (int)blockDim.x; ++i) {
-            int v = part[i];
+            const int v = part[i];
             part[i] = acc;
             acc += v;
         }
@@ -257,7 +260,7 @@ __global__ void k_scan(int *counts, int nb, int per_class, int64_t *seg)
     __syncthreads();
     int acc = part[t];
     for (int i = t * per; i < min(nb, (t + 1) * per); ++i) {
-        int v = counts[i];
+        const int v = counts[i];
         if (i % per_class == 0)
             seg[2 * (i / per_class)] = acc;
         counts[i] = acc;
@@ -269,22 +272,22 @@ __global__ void k_scan(int *counts, int nb, int per_class, int64_t *seg)
 
 __global__ void k_scatter(int64_t n, const int32_t *keys, int *cursor, int32_t *queue)
 {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const int pos = atomicAdd(&cursor[keys[i]], 1);
+    const int key = keys[i];
+    const unsigned mask = __match_any_sync(__activemask(), key);
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    int pos = 0;
+    if (lane == leader)
+        pos = atomicAdd(&cursor[key], __popc(mask));
+    pos = __shfl_sync(mask, pos, leader) + __popc(mask & ((1u << lane) - 1u));
     queue[pos] = (int32_t)i;
 }
 
 // ---------------------------------------------------------------------------
-// Smith-Waterman core: runs n pairs of (qv, rv) into d_out on c->st.
+// Smith-Waterman core
 // ---------------------------------------------------------------------------
-struct SwPlanInfo {
-    bool fast_ok;
-    int32_t max_band;
-    bool uniform_band;  // bands == nullptr
-};
-
 static int classify_band(int32_t b)
 {
     switch (b) {
@@ -296,9 +299,11 @@ static int classify_band(int32_t b)
     }
 }
 
-static int sw_core(gb2_ctx *c, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
-                   const gb2_sw_cfg *cfg, const int32_t *d_bands, const SwPlanInfo &pi, int64_t n,
-                   gb2_sw_result *d_out, int flags)
+namespace gb2 {
+
+int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
+            const gb2_sw_cfg *cfg, const int32_t *d_bands, const SwPlanInfo &pi, int64_t n,
+            gb2_sw_result *d_out, int flags)
 {
     if (n <= 0)
         return GB2_OK;
@@ -314,27 +319,29 @@ static int sw_core(gb2_ctx *c, SeqView qv, SeqView rv, int64_t qmax, int64_t rma
     const int64_t lit_stride = 3 * (2 * (int64_t)std::max(pi.max_band, 0) + 1);
     const int lit_grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)c->sm_count * 2);
     auto ensure_lit = [&]() -> int {
-        return ensure(c, c->scratch64, (size_t)lit_grid * 128 * lit_stride * sizeof(int64_t));
+        return ensure(c, x.scratch64, (size_t)lit_grid * 128 * lit_stride * sizeof(int64_t), x.st);
     };
 
+    const bool pack = pi.pack_ok && !force_literal && !(flags & GB2_FLAG_INT32);
+    const bool pack_lengths = (int64_t)match_pos * std::min(qmax, rmax) <= kPackHmax;
     // One band for every pair, pairs in input order: no planning kernels.
     if (pi.uniform_band && !batched) {
-        const int cls = (pi.fast_ok && lengths_ok && !force_literal)
-                            ? classify_band(cfg->band_width)
-                            : 0;
+        int cls = (pi.fast_ok && lengths_ok && !force_literal) ? classify_band(cfg->band_width) : 0;
+        if ((cls == 16 || cls == 32) && pack && pack_lengths)
+            cls |= kPack16;
         PairList pl{nullptr, n, nullptr, nullptr};
-        cudaEvent_t e0 = prof_begin(c, c->st);
+        cudaEvent_t e0 = prof_begin(c, x.st);
         if (cls > 0) {
             CU(c, launch_sw(cls, variant, qv, rv, p, cfg->band_width, nullptr, pl, d_out, nullptr,
-                            0, 0, c->st));
+                            0, 0, x.st));
         } else {
-            int rc = ensure_lit();
+            const int rc = ensure_lit();
             if (rc)
                 return rc;
             CU(c, launch_sw(0, 0, qv, rv, p, cfg->band_width, nullptr, pl, d_out,
-                            (int64_t *)c->scratch64.p, lit_stride, lit_grid, c->st));
+                            (int64_t *)x.scratch64.p, lit_stride, lit_grid, x.st));
         }
-        prof_end(c, e0, c->st);
+        prof_end(c, e0, x.st);
         c->launches += 1;
         return GB2_OK;
     }
@@ -342,71 +349,81 @@ static int sw_core(gb2_ctx *c, SeqView qv, SeqView rv, int64_t qmax, int64_t rma
     // Device planning: classify + count, scan, scatter.
     const int nb = kSwClasses * kLenBuckets;
     int rc;
-    if ((rc = ensure(c, c->keys, (size_t)n * 4)) || (rc = ensure(c, c->queue, (size_t)n * 4)) ||
-        (rc = ensure(c, c->counts, (size_t)nb * 4)) ||
-        (rc = ensure(c, c->seg, (size_t)kSwClasses * 2 * 8)) ||
-        (rc = ensure(c, c->counters, 64 * 4)))
+    if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
+        (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
+        (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) ||
+        (rc = ensure(c, x.seg, (size_t)kSwClasses * 2 * 8, x.st)) ||
+        (rc = ensure(c, x.counters, kCounterBytes, x.st)))
         return rc;
-    CU(c, cudaMemsetAsync(c->counts.p, 0, (size_t)nb * 4, c->st));
-    CU(c, cudaMemsetAsync(c->counters.p, 0, 64 * 4, c->st));
+    CU(c, cudaMemsetAsync(x.counts.p, 0, (size_t)nb * 4, x.st));
+    CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
     const int fast = (pi.fast_ok && !force_literal) ? 1 : 0;
     const int blocks = (int)((n + 255) / 256);
-    k_classify_sw<<<blocks, 256, 0, c->st>>>(n, qv, rv, d_bands, cfg->band_width, fast, match_pos,
-                                              (int32_t *)c->keys.p, (int *)c->counts.p);
-    k_scan<<<1, 1024, 0, c->st>>>((int *)c->counts.p, nb, kLenBuckets, (int64_t *)c->seg.p);
-    k_scatter<<<blocks, 256, 0, c->st>>>(n, (const int32_t *)c->keys.p, (int *)c->counts.p,
-                                          (int32_t *)c->queue.p);
+    k_classify_sw<<<blocks, 256, 0, x.st>>>(n, qv, rv, d_bands, cfg->band_width, fast,
+                                             pack ? 1 : 0, match_pos, (int32_t *)x.keys.p,
+                                             (int *)x.counts.p);
+    k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, kLenBuckets, (int64_t *)x.seg.p);
+    k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
+                                         (int32_t *)x.queue.p);
     CU(c, cudaGetLastError());
     c->launches += 3;
 
     // One persistent launch per class that can hold pairs; classes run
     // concurrently on the auxiliary streams.
-    static const int cls_band[kSwClasses] = {16, 32, 64, 128, 0};
-    bool need[kSwClasses] = {false, false, false, false, true};
+    static const int cls_band[kSwClasses] = {16, 32, 64, 128, 0, 16 | kPack16, 32 | kPack16};
+    static_assert(kSwClasses * kCounterStride * 4 <= (int)kCounterBytes, "counter space");
+    bool need[kSwClasses] = {false, false, false, false, true, false, false};
     if (pi.uniform_band) {
         const int cb = classify_band(cfg->band_width);
         for (int k = 0; k < 4; ++k)
             need[k] = fast && cls_band[k] == cb;
-        // every pair lands in the register class when band, config and the
-        // batch's longest sequences all qualify: skip the literal launch
+        need[5] = pack && cb == 16;
+        need[6] = pack && cb == 32;
+        // when the batch's longest sequences qualify, every pair lands in one
+        // class: skip the launches that would find nothing
+        if (need[5] || need[6]) {
+            need[0] = need[0] && !pack_lengths;
+            need[1] = need[1] && !pack_lengths;
+        }
         need[4] = !(fast && cb > 0 && lengths_ok);
     } else {
         for (int k = 0; k < 4; ++k)
             need[k] = fast && cls_band[k] <= std::max<int32_t>(pi.max_band, 0);
+        need[5] = pack && pi.max_band >= 16;
+        need[6] = pack && pi.max_band >= 32;
     }
     if (need[4] && (rc = ensure_lit()))
         return rc;
-    CU(c, cudaEventRecord(c->ev_fork, c->st));
+    CU(c, cudaEventRecord(x.ev_fork, x.st));
     int used = 0;
-    cudaEvent_t e0 = prof_begin(c, c->st);
+    cudaEvent_t e0 = prof_begin(c, x.st);
     for (int k = 0; k < kSwClasses; ++k) {
         if (!need[k])
             continue;
-        cudaStream_t s = c->aux[used % kAux];
-        CU(c, cudaStreamWaitEvent(s, c->ev_fork, 0));
-        PairList pl{(const int32_t *)c->queue.p, 0, (const int64_t *)c->seg.p + 2 * k,
-                    (int *)c->counters.p + 16 * k};
-        if (k < 4) {
+        cudaStream_t s = x.aux[used % kAux];
+        CU(c, cudaStreamWaitEvent(s, x.ev_fork, 0));
+        PairList pl{(const int32_t *)x.queue.p, 0, (const int64_t *)x.seg.p + 2 * k,
+                    (int *)x.counters.p + kCounterStride * k};
+        if (k != 4) {
             const int grid = c->sm_count * sw_blocks_per_sm(cls_band[k], variant);
             CU(c, launch_sw(cls_band[k], variant, qv, rv, p, cfg->band_width, d_bands, pl, d_out,
                             nullptr, 0, grid, s));
         } else {
             CU(c, launch_sw(0, 0, qv, rv, p, cfg->band_width, d_bands, pl, d_out,
-                            (int64_t *)c->scratch64.p, lit_stride, lit_grid, s));
+                            (int64_t *)x.scratch64.p, lit_stride, lit_grid, s));
         }
-        CU(c, cudaEventRecord(c->ev_join[used % kAux], s));
+        CU(c, cudaEventRecord(x.ev_join[used % kAux], s));
         ++used;
         c->launches += 1;
     }
     for (int i = 0; i < std::min(used, kAux); ++i)
-        CU(c, cudaStreamWaitEvent(c->st, c->ev_join[i], 0));
-    prof_end(c, e0, c->st);
+        CU(c, cudaStreamWaitEvent(x.st, x.ev_join[i], 0));
+    prof_end(c, e0, x.st);
     return GB2_OK;
 }
 
-// Validates an SW config and host band array; fills plan info.
-static int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n,
-                       int64_t qmax, int64_t rmax, SwPlanInfo &pi)
+int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n, int64_t qmax,
+                int64_t rmax, SwPlanInfo &pi)
 {
     if (!cfg)
         return set_err(c, GB2_EINVAL, "cfg is NULL");
@@ -430,11 +447,118 @@ static int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, 
                        "scores could leave the int32 range (|params| sum %lld, lengths %lld/%lld)",
                        (long long)pmax, (long long)qmax, (long long)rmax);
     pi.fast_ok = cfg->gap_extend <= 0 && cfg->gap_open + cfg->gap_extend <= 0 && cfg->mismatch <= 0;
+    const int32_t goe = cfg->gap_open + cfg->gap_extend;
+    pi.pack_ok = pi.fast_ok && cfg->mismatch >= goe && cfg->match_score >= cfg->mismatch &&
+                 cfg->match_score <= 255 && -goe <= 255 && -cfg->gap_extend <= 255;
     pi.max_band = maxb;
     pi.uniform_band = bands == nullptr;
     return GB2_OK;
 }
 
+// ---------------------------------------------------------------------------
+// WFA core
+// ---------------------------------------------------------------------------
+static int gcd_h(int a, int b)
+{
+    while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+int wfa_validate(gb2_ctx *c, const gb2_wfa_cfg *cfg, int64_t n)
+{
+    if (!cfg)
+        return set_err(c, GB2_EINVAL, "cfg is NULL");
+    if (n < 0)
+        return set_err(c, GB2_EINVAL, "n_pairs < 0");
+    if (cfg->x < 1 || cfg->e < 1 || cfg->o < 0 || cfg->max_error < 0)
+        return set_err(c, GB2_EINVAL, "WFA needs x >= 1, e >= 1, o >= 0, max_error >= 0");
+    const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
+    const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
+    if (hm > 32 || hie > 32)
+        return set_err(c, GB2_EINVAL,
+                       "WFA penalty ratios too large (max(x, o+e)/gcd and e/gcd must be <= 31)");
+    return GB2_OK;
+}
+
+int wfa_begin(gb2_ctx *c, Exec &x)
+{
+    int rc;
+    if ((rc = ensure(c, x.errflag, 64, x.st)) || (rc = ensure(c, x.work, 64, x.st)))
+        return rc;
+    CU(c, cudaMemsetAsync(x.errflag.p, 0, 64, x.st));
+    CU(c, cudaMemsetAsync(x.work.p, 0, 64, x.st));
+    return GB2_OK;
+}
+
+int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
+             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags)
+{
+    if (n <= 0)
+        return GB2_OK;
+    if (qmax >= (1ll << 30) || rmax >= (1ll << 30))
+        return set_err(c, GB2_ERANGE, "sequence longer than 2^30");
+    const WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
+    const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
+    const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
+    const int nslot = hm + 2 * hie;
+    const int64_t slot_width = ((qmax + rmax + 5) + 31) & ~int64_t(31);
+    int grid = c->sm_count * 4;
+    if ((int64_t)grid * 4 > n)
+        grid = (int)std::max<int64_t>(1, (n + 3) / 4);
+    const int64_t warps = (int64_t)grid * 4;
+    int rc;
+    if ((rc = ensure(c, x.scratch32, (size_t)warps * nslot * slot_width * 4, x.st)) ||
+        (rc = ensure(c, x.counters, kCounterBytes, x.st)))
+        return rc;
+    CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
+    PairList pl{nullptr, n, nullptr, (int *)x.counters.p};
+    if (flags & GB2_FLAG_BATCHED) {
+        const int nb = kLenBuckets;
+        if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
+            (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
+            (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) || (rc = ensure(c, x.seg, 16, x.st)))
+            return rc;
+        CU(c, cudaMemsetAsync(x.counts.p, 0, (size_t)nb * 4, x.st));
+        const int blocks = (int)((n + 255) / 256);
+        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, (int32_t *)x.keys.p,
+                                                  (int *)x.counts.p);
+        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, nb, (int64_t *)x.seg.p);
+        k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
+                                             (int32_t *)x.queue.p);
+        CU(c, cudaGetLastError());
+        c->launches += 3;
+        pl = PairList{(const int32_t *)x.queue.p, 0, (const int64_t *)x.seg.p, (int *)x.counters.p};
+    }
+    cudaEvent_t e0 = prof_begin(c, x.st);
+    CU(c, launch_wfa(0, qv, rv, p, pl, d_out, (int32_t *)x.scratch32.p, slot_width, grid,
+                     (int *)x.errflag.p, (int64_t *)x.work.p, x.st));
+    prof_end(c, e0, x.st);
+    c->launches += 1;
+    return GB2_OK;
+}
+
+int wfa_end(gb2_ctx *c, Exec &x)
+{
+    int flag = 0;
+    int64_t work = 0;
+    CU(c, cudaMemcpyAsync(&flag, x.errflag.p, 4, cudaMemcpyDeviceToHost, x.st));
+    CU(c, cudaMemcpyAsync(&work, x.work.p, 8, cudaMemcpyDeviceToHost, x.st));
+    CU(c, cudaStreamSynchronize(x.st));
+    c->work_units += work;
+    if (flag)
+        return set_err(c, GB2_EKERNEL, "WFA kernel reported a pair longer than its scratch");
+    return GB2_OK;
+}
+
+}  // namespace gb2
+
+// ---------------------------------------------------------------------------
+// blocking helpers of the context's own executor
+// ---------------------------------------------------------------------------
 static SeqView view_of(const gb2_batch *b)
 {
     return SeqView{b->d_packed, b->d_offsets, b->d_lengths, 0, std::max<int64_t>(b->n_words, 1)};
@@ -442,7 +566,7 @@ static SeqView view_of(const gb2_batch *b)
 
 static int sync_and_check(gb2_ctx *c)
 {
-    CU(c, cudaStreamSynchronize(c->st));
+    CU(c, cudaStreamSynchronize(c->x.st));
     harvest_profile(c);
     return GB2_OK;
 }
@@ -466,113 +590,16 @@ static int d2h_results(gb2_ctx *c, void *host, const void *dev, size_t bytes)
     if (bytes == 0)
         return GB2_OK;
     if (is_pinned(host)) {
-        CU(c, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->st));
+        CU(c, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->x.st));
         return sync_and_check(c);
     }
     int rc = pin_out(c, bytes);
     if (rc)
         return rc;
-    CU(c, cudaMemcpyAsync(c->pin_out, dev, bytes, cudaMemcpyDeviceToHost, c->st));
-    rc = sync_and_check(c);
-    if (rc)
+    CU(c, cudaMemcpyAsync(c->pin_out, dev, bytes, cudaMemcpyDeviceToHost, c->x.st));
+    if ((rc = sync_and_check(c)))
         return rc;
     memcpy(host, c->pin_out, bytes);
-    return GB2_OK;
-}
-
-// ---------------------------------------------------------------------------
-// WFA core
-// ---------------------------------------------------------------------------
-static int gcd_h(int a, int b)
-{
-    while (b) {
-        int t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
-static int wfa_validate(gb2_ctx *c, const gb2_wfa_cfg *cfg, int64_t n)
-{
-    if (!cfg)
-        return set_err(c, GB2_EINVAL, "cfg is NULL");
-    if (n < 0)
-        return set_err(c, GB2_EINVAL, "n_pairs < 0");
-    if (cfg->x < 1 || cfg->e < 1 || cfg->o < 0 || cfg->max_error < 0)
-        return set_err(c, GB2_EINVAL, "WFA needs x >= 1, e >= 1, o >= 0, max_error >= 0");
-    const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
-    const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
-    if (hm > 32 || hie > 32)
-        return set_err(c, GB2_EINVAL,
-                       "WFA penalty ratios too large (max(x, o+e)/gcd and e/gcd must be <= 31)");
-    return GB2_OK;
-}
-
-static int wfa_core(gb2_ctx *c, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
-                    const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags)
-{
-    if (n <= 0)
-        return GB2_OK;
-    if (qmax >= (1ll << 30) || rmax >= (1ll << 30))
-        return set_err(c, GB2_ERANGE, "sequence longer than 2^30");
-    WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
-    const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
-    const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
-    const int nslot = hm + 2 * hie;
-    const int64_t slot_width = ((qmax + rmax + 5) + 31) & ~int64_t(31);
-    const int blocks_per_sm = 4;
-    int grid = c->sm_count * blocks_per_sm;
-    const int64_t warps_needed = n;
-    if ((int64_t)grid * 4 > warps_needed)
-        grid = (int)std::max<int64_t>(1, (warps_needed + 3) / 4);
-    const int64_t warps = (int64_t)grid * 4;
-    int rc;
-    if ((rc = ensure(c, c->scratch32, (size_t)warps * nslot * slot_width * 4)) ||
-        (rc = ensure(c, c->errflag, 64)) || (rc = ensure(c, c->work, 64)) ||
-        (rc = ensure(c, c->counters, 64 * 4)))
-        return rc;
-    CU(c, cudaMemsetAsync(c->errflag.p, 0, 64, c->st));
-    CU(c, cudaMemsetAsync(c->work.p, 0, 64, c->st));
-    CU(c, cudaMemsetAsync(c->counters.p, 0, 64 * 4, c->st));
-    PairList pl{nullptr, n, nullptr, (int *)c->counters.p};
-    if (flags & GB2_FLAG_BATCHED) {
-        const int nb = kLenBuckets;
-        if ((rc = ensure(c, c->keys, (size_t)n * 4)) || (rc = ensure(c, c->queue, (size_t)n * 4)) ||
-            (rc = ensure(c, c->counts, (size_t)nb * 4)) || (rc = ensure(c, c->seg, 2 * 8)))
-            return rc;
-        CU(c, cudaMemsetAsync(c->counts.p, 0, (size_t)nb * 4, c->st));
-        const int blocks = (int)((n + 255) / 256);
-        k_classify_wfa<<<blocks, 256, 0, c->st>>>(n, qv, rv, (int32_t *)c->keys.p,
-                                                   (int *)c->counts.p);
-        k_scan<<<1, 1024, 0, c->st>>>((int *)c->counts.p, nb, nb, (int64_t *)c->seg.p);
-        k_scatter<<<blocks, 256, 0, c->st>>>(n, (const int32_t *)c->keys.p, (int *)c->counts.p,
-                                              (int32_t *)c->queue.p);
-        CU(c, cudaGetLastError());
-        c->launches += 3;
-        pl = PairList{(const int32_t *)c->queue.p, 0, (const int64_t *)c->seg.p,
-                      (int *)c->counters.p};
-    }
-    cudaEvent_t e0 = prof_begin(c, c->st);
-    CU(c, launch_wfa(0, qv, rv, p, pl, d_out, (int32_t *)c->scratch32.p, slot_width, grid,
-                     (int *)c->errflag.p, (int64_t *)c->work.p, c->st));
-    prof_end(c, e0, c->st);
-    c->launches += 1;
-    return GB2_OK;
-}
-
-static int wfa_finish(gb2_ctx *c)
-{
-    int flag = 0;
-    int64_t work = 0;
-    CU(c, cudaMemcpyAsync(&flag, c->errflag.p, 4, cudaMemcpyDeviceToHost, c->st));
-    CU(c, cudaMemcpyAsync(&work, c->work.p, 8, cudaMemcpyDeviceToHost, c->st));
-    int rc = sync_and_check(c);
-    if (rc)
-        return rc;
-    c->work_units += work;
-    if (flag)
-        return set_err(c, GB2_EKERNEL, "WFA kernel reported scratch overflow");
     return GB2_OK;
 }
 
@@ -585,9 +612,7 @@ struct HostSide {
     const int64_t *lengths;
 };
 
-static int64_t words_for(int64_t len) { return (len + 31) / 32; }
-
-// Word range [w0, w1) covering pairs [p0, p1) when offsets are monotone.
+// Word range [w0, w1) covering pairs [p0, p1) of an append-layout side.
 static void word_range(const HostSide &h, int64_t p0, int64_t p1, int64_t &w0, int64_t &w1)
 {
     w0 = h.offsets[p0];
@@ -596,39 +621,77 @@ static void word_range(const HostSide &h, int64_t p0, int64_t p1, int64_t &w0, i
         w1 = w0;
 }
 
-// True when sequences [0, n) follow add_sequence's append layout
-// (genomics/core/sequence.mojo:44-66): each starts at or after the end of
-// the previous one, so any run of pairs maps to one contiguous word range.
-static bool monotone(const HostSide &h, int64_t n, int64_t &maxlen, int64_t &maxword)
+// One pass over the host arrays of both sides: longest sequence, last word
+// touched, whether each side follows add_sequence's append layout
+// (genomics/core/sequence.mojo:44-66: every sequence starts at or after the
+// end of the previous one, so a run of pairs maps to one contiguous word
+// range) and whether any offset or length is negative.  Large batches are
+// split over a few host threads.
+struct HostScan {
+    int64_t qmaxlen = 0, rmaxlen = 0, qmaxword = 0, rmaxword = 0;
+    bool q_append = true, r_append = true, negative = false;
+};
+
+static void scan_range(const HostSide &hq, const HostSide &hr, int64_t i0, int64_t i1,
+                       HostScan &o)
 {
-    bool ok = true;
-    int64_t prev_end = 0;
-    maxlen = 0;
-    maxword = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        const int64_t o = h.offsets[i], l = h.lengths[i];
-        const int64_t e = o + words_for(l);
-        maxlen = std::max(maxlen, l);
-        maxword = std::max(maxword, e);
-        if (o < prev_end)
-            ok = false;
-        prev_end = e;
+    int64_t qprev = i0 > 0 ? hq.offsets[i0 - 1] + words_for(hq.lengths[i0 - 1]) : 0;
+    int64_t rprev = i0 > 0 ? hr.offsets[i0 - 1] + words_for(hr.lengths[i0 - 1]) : 0;
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t qo = hq.offsets[i], ql = hq.lengths[i];
+        const int64_t ro = hr.offsets[i], rl = hr.lengths[i];
+        o.negative |= (qo | ql | ro | rl) < 0;
+        const int64_t qe = qo + words_for(ql), re = ro + words_for(rl);
+        o.q_append &= qo >= qprev;
+        o.r_append &= ro >= rprev;
+        qprev = qe;
+        rprev = re;
+        o.qmaxlen = std::max(o.qmaxlen, ql);
+        o.rmaxlen = std::max(o.rmaxlen, rl);
+        o.qmaxword = std::max(o.qmaxword, qe);
+        o.rmaxword = std::max(o.rmaxword, re);
     }
-    return ok;
 }
 
-template <typename RunChunk>
-static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const int32_t *bands,
-                    int64_t n, size_t out_elem, void *out_host, int64_t chunk_pairs,
-                    RunChunk run_chunk)
+static HostScan scan_host(const HostSide &hq, const HostSide &hr, int64_t n)
 {
-    int64_t qmaxlen, rmaxlen, qmaxw, rmaxw;
-    const bool mq = monotone(hq, n, qmaxlen, qmaxw);
-    const bool mr = monotone(hr, n, rmaxlen, rmaxw);
-    for (int64_t i = 0; i < n; ++i)
-        if (hq.lengths[i] < 0 || hr.lengths[i] < 0 || hq.offsets[i] < 0 || hr.offsets[i] < 0)
-            return set_err(c, GB2_EINVAL, "negative offset or length at pair %lld", (long long)i);
-    if (!(mq && mr))
+    const int64_t per = 1 << 18;
+    const int nt = (int)std::min<int64_t>(8, (n + per - 1) / per);
+    std::vector<HostScan> parts(std::max(nt, 1));
+    if (nt <= 1) {
+        scan_range(hq, hr, 0, n, parts[0]);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t] { scan_range(hq, hr, n * t / nt, n * (t + 1) / nt, parts[t]); });
+        for (auto &x : th)
+            x.join();
+    }
+    HostScan o;
+    for (const HostScan &p : parts) {
+        o.qmaxlen = std::max(o.qmaxlen, p.qmaxlen);
+        o.rmaxlen = std::max(o.rmaxlen, p.rmaxlen);
+        o.qmaxword = std::max(o.qmaxword, p.qmaxword);
+        o.rmaxword = std::max(o.rmaxword, p.rmaxword);
+        o.q_append &= p.q_append;
+        o.r_append &= p.r_append;
+        o.negative |= p.negative;
+    }
+    return o;
+}
+
+// Chunks alternate between the context's two executors, so the kernels of
+// one chunk can fill the GPU while the previous chunk's last blocks drain;
+// copies run on their own stream ahead of both.
+template <typename RunChunk>
+static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const HostScan &sc,
+                    const int32_t *bands, int64_t n, size_t out_elem, void *out_host,
+                    int64_t chunk_pairs, RunChunk run_chunk)
+{
+    if (sc.negative)
+        return set_err(c, GB2_EINVAL, "negative offset or length");
+    const bool append = sc.q_append && sc.r_append;
+    if (!append)
         chunk_pairs = n;  // one chunk holding every word the pairs touch
     const int64_t nchunks = (n + chunk_pairs - 1) / chunk_pairs;
     int rc = GB2_OK;
@@ -637,25 +700,22 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
         return rc;
     for (int64_t ci = 0; ci < nchunks; ++ci) {
         PipeSet &ps = c->pipe[ci & 1];
+        Exec &x = (ci & 1) ? c->x2 : c->x;
         const int64_t p0 = ci * chunk_pairs, p1 = std::min(n, p0 + chunk_pairs);
         const int64_t m = p1 - p0;
-        int64_t qw0, qw1, rw0, rw1;
-        if (mq && mr) {
+        int64_t qw0 = 0, qw1 = sc.qmaxword, rw0 = 0, rw1 = sc.rmaxword;
+        if (append) {
             word_range(hq, p0, p1, qw0, qw1);
             word_range(hr, p0, p1, rw0, rw1);
-        } else {
-            qw0 = 0;
-            qw1 = qmaxw;
-            rw0 = 0;
-            rw1 = rmaxw;
         }
         const int64_t qn = std::max<int64_t>(qw1 - qw0, 1), rn = std::max<int64_t>(rw1 - rw0, 1);
         // this buffer set's previous chunk must have finished computing
         CU(c, cudaEventSynchronize(ps.done));
-        if ((rc = ensure(c, ps.qw, qn * 8)) || (rc = ensure(c, ps.rw, rn * 8)) ||
-            (rc = ensure(c, ps.qo, m * 8)) || (rc = ensure(c, ps.ql, m * 8)) ||
-            (rc = ensure(c, ps.ro, m * 8)) || (rc = ensure(c, ps.rl, m * 8)) ||
-            (rc = ensure(c, ps.out, m * out_elem)) || (bands && (rc = ensure(c, ps.bands, m * 4))))
+        if ((rc = ensure(c, ps.qw, qn * 8, x.st)) || (rc = ensure(c, ps.rw, rn * 8, x.st)) ||
+            (rc = ensure(c, ps.qo, m * 8, x.st)) || (rc = ensure(c, ps.ql, m * 8, x.st)) ||
+            (rc = ensure(c, ps.ro, m * 8, x.st)) || (rc = ensure(c, ps.rl, m * 8, x.st)) ||
+            (rc = ensure(c, ps.out, m * out_elem, x.st)) ||
+            (bands && (rc = ensure(c, ps.bands, m * 4, x.st))))
             return rc;
         if ((rc = h2d(c, ps.qw.p, hq.packed + qw0, (size_t)(qw1 - qw0) * 8, c->st_copy)) ||
             (rc = h2d(c, ps.rw.p, hr.packed + rw0, (size_t)(rw1 - rw0) * 8, c->st_copy)) ||
@@ -666,19 +726,20 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
             (bands && (rc = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy))))
             return rc;
         CU(c, cudaEventRecord(ps.copied, c->st_copy));
-        CU(c, cudaStreamWaitEvent(c->st, ps.copied, 0));
-        SeqView qv{(const uint64_t *)ps.qw.p, (const int64_t *)ps.qo.p,
-                   (const int64_t *)ps.ql.p, qw0, qn};
-        SeqView rv{(const uint64_t *)ps.rw.p, (const int64_t *)ps.ro.p,
-                   (const int64_t *)ps.rl.p, rw0, rn};
-        if ((rc = run_chunk(qv, rv, qmaxlen, rmaxlen, bands ? (const int32_t *)ps.bands.p : nullptr,
-                            m, ps.out.p)))
+        CU(c, cudaStreamWaitEvent(x.st, ps.copied, 0));
+        const SeqView qv{(const uint64_t *)ps.qw.p, (const int64_t *)ps.qo.p,
+                         (const int64_t *)ps.ql.p, qw0, qn};
+        const SeqView rv{(const uint64_t *)ps.rw.p, (const int64_t *)ps.ro.p,
+                         (const int64_t *)ps.rl.p, rw0, rn};
+        if ((rc = run_chunk(x, qv, rv, sc.qmaxlen, sc.rmaxlen,
+                            bands ? (const int32_t *)ps.bands.p : nullptr, m, ps.out.p)))
             return rc;
         void *dst = out_pinned ? (char *)out_host + p0 * out_elem
                                : (char *)c->pin_out + p0 * out_elem;
-        CU(c, cudaMemcpyAsync(dst, ps.out.p, (size_t)m * out_elem, cudaMemcpyDeviceToHost, c->st));
-        CU(c, cudaEventRecord(ps.done, c->st));
+        CU(c, cudaMemcpyAsync(dst, ps.out.p, (size_t)m * out_elem, cudaMemcpyDeviceToHost, x.st));
+        CU(c, cudaEventRecord(ps.done, x.st));
     }
+    CU(c, cudaStreamSynchronize(c->x2.st));
     if ((rc = sync_and_check(c)))
         return rc;
     if (!out_pinned)
@@ -732,21 +793,17 @@ int gb2_create(int device, gb2_ctx **out)
     gb2_ctx *c = new gb2_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
-    bool ok = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) == cudaSuccess &&
+    bool ok = exec_init(c->x) == GB2_OK && exec_init(c->x2) == GB2_OK &&
               cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
-    for (int i = 0; ok && i < kAux; ++i)
-        ok = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < 2; ++i) {
         ok = cudaMallocHost(&c->pin[i], (size_t)kPinChunk) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pipe[i].copied, cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pipe[i].done, cudaEventDisableTiming) == cudaSuccess;
         if (ok) {
-            cudaEventRecord(c->pin_ev[i], c->st);
-            cudaEventRecord(c->pipe[i].done, c->st);
+            cudaEventRecord(c->pin_ev[i], c->x.st);
+            cudaEventRecord(c->pipe[i].done, c->x.st);
         }
     }
     if (!ok) {
@@ -763,14 +820,14 @@ int gb2_destroy(gb2_ctx *c)
     if (!c)
         return GB2_EINVAL;
     cudaSetDevice(c->device);
-    if (c->st)
-        cudaStreamSynchronize(c->st);
     if (c->st_copy)
         cudaStreamSynchronize(c->st_copy);
+    if (c->x.st)
+        cudaStreamSynchronize(c->x.st);
     harvest_profile(c);
-    DevBuf *bufs[] = {&c->keys,      &c->queue,     &c->counts, &c->seg,   &c->counters,
-                      &c->out_sw,    &c->out_wfa,   &c->bands,  &c->scratch64,
-                      &c->scratch32, &c->work,      &c->errflag, &c->flush, &c->one_pair};
+    exec_free(c->x);
+    exec_free(c->x2);
+    DevBuf *bufs[] = {&c->out_sw, &c->out_wfa, &c->bands, &c->flush};
     for (DevBuf *b : bufs)
         if (b->p)
             cudaFree(b->p);
@@ -791,20 +848,10 @@ int gb2_destroy(gb2_ctx *c)
     }
     if (c->pin_out)
         cudaFreeHost(c->pin_out);
-    for (int i = 0; i < kAux; ++i) {
-        if (c->aux[i])
-            cudaStreamDestroy(c->aux[i]);
-        if (c->ev_join[i])
-            cudaEventDestroy(c->ev_join[i]);
-    }
-    if (c->ev_fork)
-        cudaEventDestroy(c->ev_fork);
     if (c->t0)
         cudaEventDestroy(c->t0);
     if (c->t1)
         cudaEventDestroy(c->t1);
-    if (c->st)
-        cudaStreamDestroy(c->st);
     if (c->st_copy)
         cudaStreamDestroy(c->st_copy);
     delete c;
@@ -818,10 +865,17 @@ int gb2_sync(gb2_ctx *c)
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     CU(c, cudaStreamSynchronize(c->st_copy));
+    CU(c, cudaStreamSynchronize(c->x2.st));
     return sync_and_check(c);
 }
 
-const char *gb2_last_error(gb2_ctx *c) { return c ? c->last_error.c_str() : "no context"; }
+const char *gb2_last_error(gb2_ctx *c)
+{
+    if (!c)
+        return "no context";
+    std::lock_guard<std::mutex> lk(c->err_mu);
+    return c->last_error.c_str();
+}
 
 int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const uint64_t *nmask,
                      const int64_t *offsets, const int64_t *lengths, int64_t count,
@@ -856,35 +910,34 @@ int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const 
         e = cudaMalloc(&b->d_offsets, sb);
     if (e == cudaSuccess)
         e = cudaMalloc(&b->d_lengths, sb);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
+    auto release = [&]() {
         cudaFree(b->d_packed);
         cudaFree(b->d_nmask);
         cudaFree(b->d_offsets);
         cudaFree(b->d_lengths);
         delete b;
+    };
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        release();
         return set_err(c, GB2_ENOMEM, "device allocation of a %lld-word batch failed",
                        (long long)n_words);
     }
     int rc = GB2_OK;
     if (n_words == 0)
-        cudaMemsetAsync(b->d_packed, 0, 8, c->st);
+        cudaMemsetAsync(b->d_packed, 0, 8, c->x.st);
     if (!rc)
-        rc = h2d(c, b->d_packed, packed, (size_t)n_words * 8, c->st);
+        rc = h2d(c, b->d_packed, packed, (size_t)n_words * 8, c->x.st);
     if (!rc && nmask)
-        rc = h2d(c, b->d_nmask, nmask, (size_t)n_words * 8, c->st);
+        rc = h2d(c, b->d_nmask, nmask, (size_t)n_words * 8, c->x.st);
     if (!rc)
-        rc = h2d(c, b->d_offsets, offsets, (size_t)count * 8, c->st);
+        rc = h2d(c, b->d_offsets, offsets, (size_t)count * 8, c->x.st);
     if (!rc)
-        rc = h2d(c, b->d_lengths, lengths, (size_t)count * 8, c->st);
+        rc = h2d(c, b->d_lengths, lengths, (size_t)count * 8, c->x.st);
     if (!rc)
         rc = sync_and_check(c);
     if (rc) {
-        cudaFree(b->d_packed);
-        cudaFree(b->d_nmask);
-        cudaFree(b->d_offsets);
-        cudaFree(b->d_lengths);
-        delete b;
+        release();
         return rc;
     }
     *out = b;
@@ -897,7 +950,7 @@ int gb2_batch_free(gb2_ctx *c, gb2_batch *b)
         return GB2_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->st);
+    cudaStreamSynchronize(c->x.st);
     cudaFree(b->d_packed);
     cudaFree(b->d_nmask);
     cudaFree(b->d_offsets);
@@ -936,16 +989,16 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
         return rc;
     if (n == 0)
         return GB2_OK;
-    if ((rc = ensure(c, c->out_sw, (size_t)n * sizeof(gb2_sw_result))))
+    if ((rc = ensure(c, c->out_sw, (size_t)n * sizeof(gb2_sw_result), c->x.st)))
         return rc;
     const int32_t *d_bands = nullptr;
     if (bands) {
-        if ((rc = ensure(c, c->bands, (size_t)n * 4)) ||
-            (rc = h2d(c, c->bands.p, bands, (size_t)n * 4, c->st)))
+        if ((rc = ensure(c, c->bands, (size_t)n * 4, c->x.st)) ||
+            (rc = h2d(c, c->bands.p, bands, (size_t)n * 4, c->x.st)))
             return rc;
         d_bands = (const int32_t *)c->bands.p;
     }
-    if ((rc = sw_core(c, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands, pi, n,
+    if ((rc = sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands, pi, n,
                       (gb2_sw_result *)c->out_sw.p, flags)))
         return rc;
     return d2h_results(c, out, c->out_sw.p, (size_t)n * sizeof(gb2_sw_result));
@@ -963,22 +1016,18 @@ int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_of
     if (n > 0 && (!q_packed || !q_offsets || !q_lengths || !r_packed || !r_offsets ||
                   !r_lengths || !out))
         return set_err(c, GB2_EINVAL, "NULL array");
-    int64_t qmax = 0, rmax = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        qmax = std::max(qmax, q_lengths[i]);
-        rmax = std::max(rmax, r_lengths[i]);
-    }
+    const HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
+    const HostScan sc = scan_host(hq, hr, std::max<int64_t>(n, 0));
     SwPlanInfo pi;
-    int rc = sw_validate(c, cfg, bands, n, qmax, rmax, pi);
+    int rc = sw_validate(c, cfg, bands, n, sc.qmaxlen, sc.rmaxlen, pi);
     if (rc || n == 0)
         return rc;
-    HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
     const int64_t chunk = std::max<int64_t>(4096, (n + 7) / 8);
-    return pipeline(c, hq, hr, bands, n, sizeof(gb2_sw_result), out, chunk,
-                    [&](SeqView qv, SeqView rv, int64_t qm, int64_t rm, const int32_t *db,
-                        int64_t m, void *dout) {
-                        return sw_core(c, qv, rv, qm, rm, cfg, db, pi, m, (gb2_sw_result *)dout,
-                                       flags);
+    return pipeline(c, hq, hr, sc, bands, n, sizeof(gb2_sw_result), out, chunk,
+                    [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm,
+                        const int32_t *db, int64_t m, void *dout) {
+                        return sw_core(c, x, qv, rv, qm, rm, cfg, db, pi, m,
+                                       (gb2_sw_result *)dout, flags);
                     });
 }
 
@@ -989,7 +1038,7 @@ int gb2_sw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_
         return GB2_EINVAL;
     if (!out || qlen < 0 || rlen < 0 || (qlen > 0 && !q_words) || (rlen > 0 && !r_words))
         return set_err(c, GB2_EINVAL, "bad pair arguments");
-    int64_t qo = 0, ro = 0;
+    const int64_t qo = 0, ro = 0;
     static const uint64_t zero = 0;
     return gb2_sw_banded_host(c, qlen ? q_words : &zero, &qo, &qlen, rlen ? r_words : &zero, &ro,
                               &rlen, cfg, nullptr, 1, out, GB2_FLAG_PLAIN);
@@ -1011,12 +1060,12 @@ int gb2_wfa_affine(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2
     int rc = wfa_validate(c, cfg, n);
     if (rc || n == 0)
         return rc;
-    if ((rc = ensure(c, c->out_wfa, (size_t)n * 4)))
+    if ((rc = ensure(c, c->out_wfa, (size_t)n * 4, c->x.st)) || (rc = wfa_begin(c, c->x)))
         return rc;
-    if ((rc = wfa_core(c, view_of(q), view_of(r), q->max_len, r->max_len, cfg, n,
+    if ((rc = wfa_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, n,
                        (int32_t *)c->out_wfa.p, flags)))
         return rc;
-    if ((rc = wfa_finish(c)))
+    if ((rc = wfa_end(c, c->x)))
         return rc;
     return d2h_results(c, out, c->out_wfa.p, (size_t)n * 4);
 }
@@ -1036,16 +1085,20 @@ int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_o
     int rc = wfa_validate(c, cfg, n);
     if (rc || n == 0)
         return rc;
-    HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
+    const HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
+    const HostScan sc = scan_host(hq, hr, n);
     const int64_t chunk = std::max<int64_t>(1024, (n + 3) / 4);
-    rc = pipeline(c, hq, hr, nullptr, n, 4, out, chunk,
-                  [&](SeqView qv, SeqView rv, int64_t qm, int64_t rm, const int32_t *,
+    if ((rc = wfa_begin(c, c->x)) || (rc = wfa_begin(c, c->x2)))
+        return rc;
+    rc = pipeline(c, hq, hr, sc, nullptr, n, 4, out, chunk,
+                  [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, const int32_t *,
                       int64_t m, void *dout) {
-                      return wfa_core(c, qv, rv, qm, rm, cfg, m, (int32_t *)dout, flags);
+                      return wfa_core(c, x, qv, rv, qm, rm, cfg, m, (int32_t *)dout, flags);
                   });
     if (rc)
         return rc;
-    return wfa_finish(c);
+    const int r1 = wfa_end(c, c->x), r2 = wfa_end(c, c->x2);
+    return r1 ? r1 : r2;
 }
 
 int gb2_wfa_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
@@ -1055,7 +1108,7 @@ int gb2_wfa_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64
         return GB2_EINVAL;
     if (!out || qlen < 0 || rlen < 0 || (qlen > 0 && !q_words) || (rlen > 0 && !r_words))
         return set_err(c, GB2_EINVAL, "bad pair arguments");
-    int64_t qo = 0, ro = 0;
+    const int64_t qo = 0, ro = 0;
     static const uint64_t zero = 0;
     return gb2_wfa_affine_host(c, qlen ? q_words : &zero, &qo, &qlen, rlen ? r_words : &zero, &ro,
                                &rlen, cfg, 1, out, GB2_FLAG_PLAIN);
@@ -1086,7 +1139,7 @@ int gb2_timer_start(gb2_ctx *c)
     if (!c)
         return GB2_EINVAL;
     cudaSetDevice(c->device);
-    CU(c, cudaEventRecord(c->t0, c->st));
+    CU(c, cudaEventRecord(c->t0, c->x.st));
     return GB2_OK;
 }
 
@@ -1095,7 +1148,7 @@ int gb2_timer_stop(gb2_ctx *c, float *ms)
     if (!c || !ms)
         return GB2_EINVAL;
     cudaSetDevice(c->device);
-    CU(c, cudaEventRecord(c->t1, c->st));
+    CU(c, cudaEventRecord(c->t1, c->x.st));
     CU(c, cudaEventSynchronize(c->t1));
     CU(c, cudaEventElapsedTime(ms, c->t0, c->t1));
     return GB2_OK;
@@ -1107,14 +1160,16 @@ int gb2_stats(gb2_ctx *c, double *kernel_ms, int64_t *launches, int64_t *work_un
         return GB2_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    CU(c, cudaStreamSynchronize(c->st));
+    CU(c, cudaStreamSynchronize(c->x.st));
     harvest_profile(c);
-    if (kernel_ms)
+    if (kernel_ms) {
+        std::lock_guard<std::mutex> pk(c->prof_mu);
         *kernel_ms = c->kernel_ms;
+    }
     if (launches)
-        *launches = c->launches;
+        *launches = c->launches.load();
     if (work_units)
-        *work_units = c->work_units;
+        *work_units = c->work_units.load();
     return GB2_OK;
 }
 
@@ -1124,9 +1179,12 @@ int gb2_stats_reset(gb2_ctx *c)
         return GB2_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    CU(c, cudaStreamSynchronize(c->st));
+    CU(c, cudaStreamSynchronize(c->x.st));
     harvest_profile(c);
-    c->kernel_ms = 0;
+    {
+        std::lock_guard<std::mutex> pk(c->prof_mu);
+        c->kernel_ms = 0;
+    }
     c->launches = 0;
     c->work_units = 0;
     return GB2_OK;
@@ -1136,7 +1194,6 @@ int gb2_set_profiling(gb2_ctx *c, int enable)
 {
     if (!c)
         return GB2_EINVAL;
-    std::lock_guard<std::mutex> lk(c->mu);
     c->profiling = enable != 0;
     return GB2_OK;
 }
@@ -1148,29 +1205,28 @@ int gb2_flush_l2(gb2_ctx *c)
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     const size_t bytes = 256ull << 20;  // twice the 126 MB L2
-    int rc = ensure(c, c->flush, bytes);
+    const int rc = ensure(c, c->flush, bytes, c->x.st);
     if (rc)
         return rc;
-    CU(c, cudaMemsetAsync(c->flush.p, c->launches & 0xff, bytes, c->st));
+    CU(c, cudaMemsetAsync(c->flush.p, (int)(c->launches.load() & 0xff), bytes, c->x.st));
     return GB2_OK;
 }
 
 int gb2_int_peak(gb2_ctx *c, int kind, double *gops)
 {
-    if (!c || !gops || kind < 0 || kind > 7)
+    if (!c || !gops || kind < 0 || kind > 12)
         return GB2_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    int rc = ensure(c, c->work, 64);
+    const int rc = ensure(c, c->x.work, 64, c->x.st);
     if (rc)
         return rc;
-    CU(c, cudaMemsetAsync(c->work.p, 0, 64, c->st));
+    CU(c, cudaMemsetAsync(c->x.work.p, 0, 64, c->x.st));
     const int block = 256, grid = c->sm_count * 8, iters = 4096;
-    // warm-up, then timed
-    CU(c, launch_int_peak(kind, grid, block, 64, (uint32_t *)c->work.p, c->st));
-    CU(c, cudaEventRecord(c->t0, c->st));
-    CU(c, launch_int_peak(kind, grid, block, iters, (uint32_t *)c->work.p, c->st));
-    CU(c, cudaEventRecord(c->t1, c->st));
+    CU(c, launch_int_peak(kind, grid, block, 64, (uint32_t *)c->x.work.p, c->x.st));
+    CU(c, cudaEventRecord(c->t0, c->x.st));
+    CU(c, launch_int_peak(kind, grid, block, iters, (uint32_t *)c->x.work.p, c->x.st));
+    CU(c, cudaEventRecord(c->t1, c->x.st));
     CU(c, cudaEventSynchronize(c->t1));
     float ms = 0.f;
     CU(c, cudaEventElapsedTime(&ms, c->t0, c->t1));

@@ -67,6 +67,9 @@ struct SwParams {
     int32_t match, mismatch, go, ge;
 };
 
+// band_class flag selecting the packed int16x2 kernel (bands 16 and 32).
+constexpr int kPack16 = 0x100;
+
 // Smith-Waterman launch over a list of pair indices (queue == nullptr means
 // pairs [0, n)).  `bands` (device, may be nullptr) overrides `band`.
 // band_class: 16, 32, 64, 128 for the register kernels, 0 for the literal

@@ -1,0 +1,126 @@
+// runtime.cuh -- host runtime types shared by api.cu and server.cu (not installed).
+#pragma once
+#include <atomic>
+#include <cstdarg>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gb2_internal.cuh"
+
+namespace gb2 {
+
+constexpr int kAux = 4;            // auxiliary streams for concurrent band classes
+constexpr int kSwClasses = 7;      // 16, 32, 64, 128, literal, packed 16, packed 32
+constexpr int kLenBuckets = 1024;  // length buckets per class
+constexpr int64_t kPinChunk = 32ll << 20;
+constexpr int64_t kPackHmax = 511;  // packed kernel: H*128 + column fits 16 bits
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+// An executor: one stream (plus auxiliary streams for concurrent band
+// classes) and the planning / scratch buffers its launches use.  Work on one
+// executor is ordered; separate executors can overlap on the device.
+struct Exec {
+    cudaStream_t st = nullptr;
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
+    DevBuf keys, queue, counts, seg, counters, scratch64, scratch32, work, errflag;
+};
+
+// One set of device buffers of the end-to-end pipeline.
+struct PipeSet {
+    DevBuf qw, rw, qo, ql, ro, rl, bands, out;
+    cudaEvent_t copied = nullptr, done = nullptr;
+};
+
+struct SwPlanInfo {
+    bool fast_ok;       // the register kernels apply (sign conditions on the scores)
+    bool pack_ok;       // the packed int16x2 kernel applies (scores also small)
+    int32_t max_band;
+    bool uniform_band;  // no per-pair bands
+};
+
+}  // namespace gb2
+
+struct gb2_batch {
+    uint64_t *d_packed = nullptr;
+    uint64_t *d_nmask = nullptr;
+    int64_t *d_offsets = nullptr;
+    int64_t *d_lengths = nullptr;
+    int64_t count = 0, n_words = 0, max_len = 0;
+    gb2_ctx *owner = nullptr;
+};
+
+struct gb2_ctx {
+    int device = 0;
+    int sm_count = 148;
+    gb2::Exec x;                  // the executor of the blocking entry points
+    gb2::Exec x2;                 // second executor: the host pipeline alternates chunks
+    cudaStream_t st_copy = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::mutex mu;                // serialises the entry points of this context
+    std::mutex err_mu;
+    std::string last_error;
+    gb2::DevBuf out_sw, out_wfa, bands, flush;
+    void *pin[2] = {nullptr, nullptr};  // pinned staging halves for pageable uploads
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+    std::mutex pin_mu;
+    void *pin_out = nullptr;
+    size_t pin_out_cap = 0;
+    gb2::PipeSet pipe[2];
+    // statistics
+    std::atomic<bool> profiling{false};
+    std::mutex prof_mu;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pending;
+    double kernel_ms = 0.0;
+    std::atomic<int64_t> launches{0};
+    std::atomic<int64_t> work_units{0};
+};
+
+namespace gb2 {
+
+int set_err(gb2_ctx *c, int code, const char *fmt, ...);
+
+#define GB2_CU(ctx, call)                                                                  \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return ::gb2::set_err((ctx),                                                   \
+                                  e_ == cudaErrorMemoryAllocation ? GB2_ENOMEM : GB2_ECUDA, \
+                                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                                  __LINE__);                                               \
+    } while (0)
+
+int exec_init(Exec &x);
+void exec_free(Exec &x);
+// Grows b to at least `bytes`; an existing buffer is freed after `st` drains.
+int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st);
+bool is_pinned(const void *p);
+// Host-to-device copy on st: pinned sources by DMA, pageable ones through the
+// context's two pinned staging halves.
+int h2d(gb2_ctx *c, void *dst, const void *src, size_t bytes, cudaStream_t st);
+int64_t words_for(int64_t len);
+void harvest_profile(gb2_ctx *c);
+
+int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n, int64_t qmax,
+                int64_t rmax, SwPlanInfo &pi);
+// Enqueues Smith-Waterman for n pairs of (qv, rv) on executor x; results to d_out.
+int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
+            const gb2_sw_cfg *cfg, const int32_t *d_bands, const SwPlanInfo &pi, int64_t n,
+            gb2_sw_result *d_out, int flags);
+int wfa_validate(gb2_ctx *c, const gb2_wfa_cfg *cfg, int64_t n);
+// Clears the WFA error flag and work counter of x (once per call, before the
+// first wfa_core of that call).
+int wfa_begin(gb2_ctx *c, Exec &x);
+int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
+             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags);
+// Reads back x's WFA error flag and work counter (synchronises x's stream),
+// folds the work into the context's statistics and turns the flag into a status.
+int wfa_end(gb2_ctx *c, Exec &x);
+
+}  // namespace gb2

@@ -237,6 +237,226 @@ sw_band_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__r
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed int16x2 kernel (sw_pack16_kernel<B>): one thread per pair, two cells
+// per 32-bit register, one DPX instruction advancing both.
+//
+// Band columns 0..B live in the low halves, columns B+1..2B in the high
+// halves of R = B+1 registers; the high half of the last register is a
+// padding column held at H = 0 (it is the out-of-band "up" of column 2B).
+// At step t the low halves hold row t and the high halves row t-1, so the
+// two cells of a register are never each other's neighbours:
+//   low  (t, h):      diag/up from the same half of registers h, h+1 of step
+//                     t-1; up of h = B is the high half of register 0 (row
+//                     t-1, column B+1), computed earlier in this step;
+//   high (t-1, B+1+h): diag/up from the same half of step t-1; left of h = 0
+//                     is the low half of register B of step t-1 (row t-1,
+//                     column B).
+// Values: registers hold H; the E chain is carried as E - (go+ge), so
+//   E' = max(E'_left + ge, H_up),
+//   H  = max(H_diag + sub - (go+ge), E', H_left, -(go+ge)) + (go+ge).
+// Without the max(E, 0) clamp E differs from the reference's E only in
+// non-positive values, which never reach H (H takes max(.., 0)); the
+// -1000000 start of the chain at column 0 becomes a large negative value.
+// Bits: H <= 511 in every cell (the host checks match*min(qlen, rlen)), all
+// terms stay inside int16, the first-maximum key H*128 + (127-column) fits
+// an unsigned 16-bit half, and the per-half subtract of |go+ge| cannot
+// borrow because H' >= |go+ge|.  The substitution score comes from the
+// equality bits of both rows: s = eqL | eqH << 16, sub - (go+ge) =
+// s*(match-mismatch) + (mismatch-(go+ge)) with mismatch >= go+ge, so the
+// multiply-add never carries between halves.
+// ---------------------------------------------------------------------------
+// One step of sw_pack16_kernel over all R registers.  MASK = false when every
+// cell of the step lies inside the matrix (the common case); MASK = true
+// zeroes the first-maximum keys of cells past the query or reference end.
+// Returns the packed row keys: low half row t, high half row t-1.
+template <int B, bool MASK>
+__device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const uint64_t *eqc,
+                                                 const uint64_t *bw, uint32_t &e_last, int limL,
+                                                 int limH, uint32_t GE2, uint32_t NG2,
+                                                 uint32_t GOE_SUB, uint32_t MMG2, uint32_t DM)
+{
+    constexpr int NL = B + 1, R = NL;
+    const uint32_t SENT = 0x0000C000u;
+    uint32_t hl = Hr[R - 1] << 16;                    // low: band edge 0; high: H(t-1, B)
+    uint32_t el = __byte_perm(SENT, e_last, 0x5410);  // low: chain start; high: E'(t-1, B)
+    uint32_t h0new = 0;
+    uint32_t rk = 0, kpend = 0;
+#pragma unroll
+    for (int h = 0; h < R; ++h) {
+        const int k = h >> 4, j = h & 15;
+        const uint32_t a32 = (k & 1) ? (uint32_t)eqc[k >> 1] : (uint32_t)(eqc[k >> 1] >> 32);
+        const uint32_t b32 = (k & 1) ? (uint32_t)bw[k >> 1] : (uint32_t)(bw[k >> 1] >> 32);
+        const uint32_t wsel = (j < 8) ? __byte_perm(a32, b32, 0x7632) : __byte_perm(a32, b32, 0x5410);
+        const int pos = (j < 8) ? (14 - 2 * j) : (30 - 2 * j);
+        const uint32_t sub = ((wsel >> pos) & 0x00010001u) * DM + MMG2;
+        const uint32_t up = (h + 1 < R) ? Hr[h + 1 < R ? h + 1 : h] : (h0new >> 16);
+        const uint32_t e = __viaddmax_s16x2(el, GE2, up);
+        const uint32_t tt = __vimax3_s16x2(e, hl, NG2);
+        uint32_t hn = __viaddmax_s16x2(Hr[h], sub, tt) - GOE_SUB;
+        if (h == R - 1)
+            hn &= 0x0000FFFFu;  // padding column stays 0
+        if (h == 0)
+            h0new = hn;
+        Hr[h] = hn;
+        hl = hn;
+        el = e;
+        uint32_t key = hn * 128u + (((uint32_t)(127 - h)) | ((uint32_t)(127 - NL - h) << 16));
+        if (MASK)
+            key &= (h < limL ? 0x0000FFFFu : 0u) | (h < limH ? 0xFFFF0000u : 0u);
+        if (h & 1)
+            rk = __vimax3_u16x2(rk, kpend, key);
+        else
+            kpend = key;
+    }
+    if ((R - 1) % 2 == 0)
+        rk = __vimax3_u16x2(rk, kpend, kpend);
+    e_last = el;
+    return rk;
+}
+
+template <int B>
+__global__ void __launch_bounds__(128)
+sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__restrict__ out)
+{
+    constexpr int W = 2 * B + 1;
+    constexpr int NL = B + 1;           // columns in low halves
+    constexpr int R = NL;               // registers
+    constexpr int NWIN = (W + 31) / 32; // 64-bit eq words of one row
+    constexpr int SHIFT = 2 * NL;       // bits between column h and column NL+h
+    constexpr int SW_ = SHIFT / 64, SB_ = SHIFT % 64;
+    static_assert(W <= 127, "column index must fit the key");
+
+    int64_t n;
+    const int32_t *__restrict__ queue = pairs_resolve(pl, n);
+    int *const queue_counter = pl.counter;
+    const int lane = threadIdx.x & 31;
+    const int warps_per_block = blockDim.x >> 5;
+    const int64_t warp_global = (int64_t)blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+    const int64_t warps_total = (int64_t)gridDim.x * warps_per_block;
+
+    const int32_t goe = p.go + p.ge;  // <= 0
+    const uint32_t GE2 = ((uint32_t)(uint16_t)p.ge) * 0x00010001u;
+    const uint32_t NG2 = ((uint32_t)(uint16_t)(-goe)) * 0x00010001u;
+    const uint32_t GOE_SUB = (uint32_t)(-goe) * 0x00010001u;
+    const uint32_t MMG2 = (uint32_t)(p.mismatch - goe) * 0x00010001u;
+    const uint32_t DM = (uint32_t)(p.match - p.mismatch);
+    const uint32_t SENT = 0x0000C000u;  // -16384 in the low half
+
+    int64_t base = warp_global * 32;
+    for (;;) {
+        if (queue_counter) {
+            int64_t b0 = 0;
+            if (lane == 0)
+                b0 = atomicAdd(queue_counter, 32);
+            base = __shfl_sync(0xffffffffu, b0, 0);
+        }
+        if (base >= n)
+            break;
+        const int64_t slot = base + lane;
+        if (slot < n) {
+            const int64_t pi = queue ? (int64_t)queue[slot] : slot;
+            const int64_t qoff = q.offsets[pi] - q.word_base;
+            const int64_t roff = r.offsets[pi] - r.word_base;
+            const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
+            uint32_t Hr[R];
+#pragma unroll
+            for (int h = 0; h < R; ++h)
+                Hr[h] = 0;
+            uint64_t eqp[NWIN + 1];
+#pragma unroll
+            for (int i = 0; i <= NWIN; ++i)
+                eqp[i] = 0;
+            uint32_t e_last = SENT;
+            uint32_t saved_lowkey = 0;
+            int32_t best = 0, bq = 0, bc = 0;
+            const int steps = qlen > 0 ? qlen + 1 : 0;
+            for (int t = 0; t < steps; ++t) {
+                // equality bits of row t against its window r[t-B .. t+B]
+                uint64_t eqc[NWIN + 1];
+                eqc[NWIN] = 0;
+                if (t < qlen) {
+                    const uint64_t qw = __ldg(q.packed + qoff + (t >> 5));
+                    const uint64_t qrep = ((qw >> (62 - 2 * (t & 31))) & 3u) * 0x5555555555555555ull;
+                    const int64_t ri0 = (int64_t)t - B;
+                    const int64_t w = roff + (ri0 >> 5);
+                    const int sh = (int)(ri0 & 31) * 2;
+                    uint64_t words[NWIN + 1];
+#pragma unroll
+                    for (int i = 0; i <= NWIN; ++i) {
+                        int64_t wi = w + i;
+                        wi = wi < 0 ? 0 : (wi >= r.n_words ? r.n_words - 1 : wi);
+                        words[i] = __ldg(r.packed + wi);
+                    }
+#pragma unroll
+                    for (int i = 0; i < NWIN; ++i) {
+                        const uint64_t win =
+                            sh ? ((words[i] << sh) | (words[i + 1] >> (64 - sh))) : words[i];
+                        const uint64_t x = win ^ qrep;
+                        eqc[i] = ~(x | (x >> 1)) & 0x5555555555555555ull;
+                    }
+                    if (ri0 < 0) {  // columns before the reference start never match
+                        const int64_t nneg = -ri0;
+#pragma unroll
+                        for (int i = 0; i < NWIN; ++i) {
+                            const int64_t cnt = nneg - 32 * i;
+                            if (cnt >= 32)
+                                eqc[i] = 0;
+                            else if (cnt > 0)
+                                eqc[i] &= (~0ull) >> (2 * cnt);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NWIN; ++i)
+                        eqc[i] = 0;
+                }
+                // previous row's bits, shifted so column NL+h sits where column h does
+                uint64_t bw[NWIN];
+#pragma unroll
+                for (int i = 0; i < NWIN; ++i) {
+                    const uint64_t a = (i + SW_ <= NWIN) ? eqp[i + SW_] : 0;
+                    const uint64_t b = (i + SW_ + 1 <= NWIN) ? eqp[i + SW_ + 1] : 0;
+                    bw[i] = SB_ ? ((a << SB_) | (b >> (64 - SB_))) : a;
+                }
+                // does any cell of this step fall outside the matrix?
+                const bool full = (t >= 1) && (t < qlen) && (t + B - 1 < rlen);
+                int limL = 0, limH = 0;
+                if (!full) {
+                    if (t < qlen)
+                        limL = max(0, min(NL, rlen - (t - B)));
+                    if (t >= 1 && t - 1 < qlen)
+                        limH = max(0, min(R, rlen - (t - 1 - B + NL)));
+                }
+                const uint32_t rk =
+                    full ? pack16_cells<B, false>(Hr, eqc, bw, e_last, 0, 0, GE2, NG2, GOE_SUB,
+                                                  MMG2, DM)
+                         : pack16_cells<B, true>(Hr, eqc, bw, e_last, limL, limH, GE2, NG2,
+                                                 GOE_SUB, MMG2, DM);
+                // row t-1 is complete: its first half came one step earlier
+                const uint32_t highkey = rk >> 16, lowkey = rk & 0xFFFFu;
+                const uint32_t rowkey = max(saved_lowkey, highkey);
+                if ((int32_t)(rowkey >> 7) > best) {
+                    best = (int32_t)(rowkey >> 7);
+                    bq = t - 1;
+                    bc = 127 - (int32_t)(rowkey & 127u);
+                }
+                saved_lowkey = lowkey;
+#pragma unroll
+                for (int i = 0; i < NWIN; ++i)
+                    eqp[i] = eqc[i];
+            }
+            gb2_sw_result res;
+            res.score = best;
+            res.query_end = best > 0 ? bq : 0;
+            res.ref_end = best > 0 ? bq - B + bc : 0;
+            out[pi] = res;
+        }
+        if (!queue_counter)
+            base += warps_total * 32;
+    }
+}
+
 // Literal per-pair kernel: one thread per pair, int64 arithmetic, rows in
 // global scratch.  Statement order follows align_cpu.mojo:239-309 exactly,
 // so it is exact for every configuration and band.
@@ -330,9 +550,19 @@ static int occ_band()
     return nb > 0 ? nb : 1;
 }
 
+template <int B>
+static int occ_pack16()
+{
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sw_pack16_kernel<B>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
 int sw_blocks_per_sm(int band_class, int variant)
 {
     switch (band_class) {
+    case 16 | kPack16: return occ_pack16<16>();
+    case 32 | kPack16: return occ_pack16<32>();
     case 16: return variant == 1 ? occ_band<16, 2, 17>() : occ_band<16, 1, 33>();
     case 32:
         return variant == 1 ? occ_band<32, 2, 33>()
@@ -347,6 +577,8 @@ int sw_pairs_per_block(int band_class, int variant)
 {
     int G = 1;
     switch (band_class) {
+    case 16 | kPack16:
+    case 32 | kPack16: return 128;
     case 16: G = variant == 1 ? 2 : 1; break;
     case 32: G = variant == 1 ? 2 : (variant == 2 ? 4 : 1); break;
     case 64: G = variant == 1 ? 4 : 2; break;
@@ -362,6 +594,20 @@ cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParam
                       int64_t scratch_stride, int grid, cudaStream_t st)
 {
     switch (band_class) {
+    case 16 | kPack16:
+    case 32 | kPack16: {
+        int g = grid;
+        if (g <= 0) {
+            if (pl.seg || pl.n <= 0)
+                return pl.n <= 0 && !pl.seg ? cudaSuccess : cudaErrorInvalidValue;
+            g = (int)((pl.n + 127) / 128);
+        }
+        if (band_class == (16 | kPack16))
+            sw_pack16_kernel<16><<<g, 128, 0, st>>>(q, r, p, pl, out);
+        else
+            sw_pack16_kernel<32><<<g, 128, 0, st>>>(q, r, p, pl, out);
+        return cudaGetLastError();
+    }
     case 16:
         if (variant == 1)
             return launch_band<16, 2, 17>(q, r, p, pl, out, grid, st);

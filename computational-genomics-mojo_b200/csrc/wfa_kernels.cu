@@ -364,11 +364,41 @@ __global__ void int_peak_kernel(int kind, int iters, uint32_t *sink)
             for (int i = 0; i < 8; ++i)
                 a[i] = a[i] * c1 + a[(i + 1) & 7];
         break;
-    default:
+    case 7:
         for (int it = 0; it < iters; ++it)
 #pragma unroll
             for (int i = 0; i < 8; ++i)
                 a[i] = __shfl_xor_sync(0xffffffffu, a[i], 1) + c1;
+        break;
+    case 8:
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                a[i] = __vimax3_s16x2(a[i], a[(i + 1) & 7], a[(i + 2) & 7]);
+        break;
+    case 9:
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                a[i] = __vimax3_u16x2(a[i], a[(i + 1) & 7], a[(i + 2) & 7]);
+        break;
+    case 10:
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                a[i] = __byte_perm(a[i], a[(i + 1) & 7], 0x7632);
+        break;
+    case 11:
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                a[i] = __viaddmax_s16x2_relu(a[i], c1, a[(i + 1) & 7]);
+        break;
+    default:
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                a[i] = __vimax_s16x2_relu(a[i], a[(i + 1) & 7]);
         break;
     }
     uint32_t s = 0;

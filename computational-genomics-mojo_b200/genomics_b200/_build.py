@@ -16,7 +16,7 @@ INCLUDE = os.path.join(REPO_ROOT, "include")
 LIB = os.path.join(LIBDIR, "libgenomics_b200.so")
 SYNTH = os.path.join(LIBDIR, "libgenomics_synth.so")
 
-CU_SOURCES = ["api.cu", "sw_kernels.cu", "wfa_kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["api.cu", "sw_kernels.cu", "wfa_kernels.cu", "noalloc.cu", "server.cu", "pack.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -34,7 +34,8 @@ def _nvcc():
 
 def _deps():
     deps = [os.path.join(CSRC, f) for f in CU_SOURCES]
-    deps += [os.path.join(CSRC, "gb2_internal.cuh"), os.path.join(INCLUDE, "genomics_b200.h")]
+    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    deps.append(os.path.join(INCLUDE, "genomics_b200.h"))
     return deps
 
 

@@ -47,6 +47,27 @@ class WfaCfg(ctypes.Structure):
     _fields_ = [("x", c_i32), ("o", c_i32), ("e", c_i32), ("max_error", c_i32)]
 
 
+class Request(ctypes.Structure):
+    """gb2_request: one serving request (a batch of SW / WFA pairs)."""
+    _fields_ = [("n_pairs", c_i64),
+                ("q_packed", vp), ("q_offsets", vp), ("q_lengths", vp),
+                ("r_packed", vp), ("r_offsets", vp), ("r_lengths", vp),
+                ("kinds", vp), ("bands", vp),
+                ("sw_cfg", SwCfg), ("wfa_cfg", WfaCfg),
+                ("sw_out", vp), ("wfa_out", vp)]
+
+
+class ServerCfg(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", c_i64), ("max_inflight_groups", c_i32),
+                ("max_group_pairs", c_i32), ("flags", c_i32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", c_i64), ("completed", c_i64), ("failed", c_i64),
+                ("pairs_completed", c_i64), ("groups_launched", c_i64),
+                ("inflight_bytes", c_i64), ("peak_inflight_bytes", c_i64)]
+
+
 # (name, restype, argtypes) for every entry point of include/genomics_b200.h
 SIGNATURES = [
     ("gb2_version", ctypes.c_int, []),
@@ -58,6 +79,8 @@ SIGNATURES = [
     ("gb2_batch_upload", ctypes.c_int, [vp, vp, c_i64, vp, vp, vp, c_i64, P(vp)]),
     ("gb2_batch_free", ctypes.c_int, [vp, vp]),
     ("gb2_batch_info", ctypes.c_int, [vp, P(c_i64), P(c_i64)]),
+    ("gb2_batch_from_ascii", ctypes.c_int, [vp, vp, c_i64, vp, vp, c_i64, P(vp)]),
+    ("gb2_batch_download", ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
     ("gb2_sw_banded", ctypes.c_int, [vp, vp, vp, P(SwCfg), vp, c_i64, vp, ctypes.c_int]),
     ("gb2_sw_banded_host", ctypes.c_int,
      [vp, vp, vp, vp, vp, vp, vp, P(SwCfg), vp, c_i64, vp, ctypes.c_int]),
@@ -68,6 +91,12 @@ SIGNATURES = [
     ("gb2_wfa_pair", ctypes.c_int, [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32)]),
     ("gb2_wfa_affine_noalloc", ctypes.c_int,
      [vp, c_i64, vp, vp, vp, c_i64, vp, vp, c_i64, c_i64, P(WfaCfg), c_i64, vp, vp]),
+    ("gb2_server_start", ctypes.c_int, [vp, P(ServerCfg), P(vp)]),
+    ("gb2_server_submit", ctypes.c_int, [vp, P(Request), P(ctypes.c_uint64)]),
+    ("gb2_server_poll", ctypes.c_int, [vp, ctypes.c_uint64, P(ctypes.c_int)]),
+    ("gb2_server_wait", ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_double)]),
+    ("gb2_server_stats_get", ctypes.c_int, [vp, P(ServerStats)]),
+    ("gb2_server_stop", ctypes.c_int, [vp]),
     ("gb2_host_alloc", ctypes.c_int, [c_i64, P(vp)]),
     ("gb2_host_free", ctypes.c_int, [vp]),
     ("gb2_timer_start", ctypes.c_int, [vp]),

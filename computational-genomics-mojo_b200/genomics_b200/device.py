@@ -91,6 +91,33 @@ class GenomicsDevice:
                                             _ptr(ln), ln.size, ctypes.byref(h)))
         return DeviceBatch(self, h, int(ln.size), int(packed.size))
 
+    def batch_from_ascii(self, seqs) -> DeviceBatch:
+        """Packs ASCII sequences on the device (SequenceBatch.add_sequence,
+        genomics/core/sequence.mojo:38-66); returns the resident batch."""
+        bs = [s.encode() if isinstance(s, str) else bytes(s) for s in seqs]
+        lengths = np.fromiter((len(b) for b in bs), np.int64, len(bs))
+        starts = np.zeros(len(bs), np.int64)
+        if len(bs) > 1:
+            np.cumsum(lengths[:-1], out=starts[1:])
+        buf = np.frombuffer(b"".join(bs) or b"\0", np.uint8)
+        h = ctypes.c_void_p()
+        self._check(self.L.gb2_batch_from_ascii(self.ctx, _ptr(buf), int(lengths.sum()),
+                                                _ptr(starts), _ptr(lengths), len(bs),
+                                                ctypes.byref(h)))
+        count, words = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.L.gb2_batch_info(h, ctypes.byref(count), ctypes.byref(words)))
+        return DeviceBatch(self, h, count.value, words.value)
+
+    def download_batch(self, b: DeviceBatch) -> SequenceBatch:
+        """Copies a resident batch back into a host SequenceBatch."""
+        p = np.zeros(max(b.n_words, 1), np.uint64)
+        m = np.zeros(max(b.n_words, 1), np.uint64)
+        o = np.zeros(max(b.count, 1), np.int64)
+        ln = np.zeros(max(b.count, 1), np.int64)
+        self._check(self.L.gb2_batch_download(self.ctx, b.handle, _ptr(p), _ptr(m), _ptr(o),
+                                              _ptr(ln)))
+        return SequenceBatch.from_arrays(p[:b.n_words], m[:b.n_words], o[:b.count], ln[:b.count])
+
     # -- Smith-Waterman -------------------------------------------------------------
     def sw_banded(self, q, r, cfg, bands=None, n_pairs=None, batched=True, flags=0, out=None):
         """Batched smith_waterman_banded over pairs (q[i], r[i]).

@@ -111,6 +111,19 @@ int gb2_batch_free(gb2_ctx *ctx, gb2_batch *batch);
 /* Number of sequences / packed words held by a batch. */
 int gb2_batch_info(const gb2_batch *batch, int64_t *count, int64_t *n_words);
 
+/* Device-side SequenceBatch.add_sequence (genomics/core/sequence.mojo:38-66)
+   for a whole batch: sequence i is ascii[starts[i] .. starts[i]+lengths[i]);
+   it is copied to the device once and packed there (2-bit MSB-first words,
+   non-ACGT stored as A and flagged in the NMask words), sequences appended
+   in order.  The batch keeps its NMask words. */
+int gb2_batch_from_ascii(gb2_ctx *ctx, const uint8_t *ascii, int64_t ascii_bytes,
+                         const int64_t *starts, const int64_t *lengths, int64_t count,
+                         gb2_batch **out);
+/* Copies a device batch back (any pointer may be NULL; sizes from
+   gb2_batch_info). */
+int gb2_batch_download(gb2_ctx *ctx, const gb2_batch *batch, uint64_t *packed,
+                       uint64_t *nmask, int64_t *offsets, int64_t *lengths);
+
 /* ---- batched banded Smith-Waterman --------------------------------------------
  * Pair i = (query i of q, reference i of r), as launch_banded_sw
  * (genomics/gpu/align_gpu.mojo:460-492).  `bands` (host, may be NULL) gives
@@ -185,6 +198,61 @@ int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
                            const gb2_wfa_cfg *cfg, int64_t n_pairs,
                            int32_t *out_cost, void *stream);
 
+/* ---- serving: continuous batching of alignment requests ----------------------------
+ * A request is a batch of pairs; each pair is Smith-Waterman or WFA.  Requests
+ * are admitted in arrival order while the device memory they need fits the
+ * server's HBM budget; admitted requests are grouped and launched as soon as
+ * one of the server's executors is free, so requests that arrive while others
+ * run on the GPU start before those finish and their work overlaps on the
+ * device.  Results are exactly those of gb2_sw_banded / gb2_wfa_affine on the
+ * same pairs, whatever else is in flight. */
+typedef struct {
+    int64_t n_pairs;
+    /* host SequenceBatch arrays of the queries and references (pair i = q i, r i);
+       they and the output arrays must stay valid until the request is done */
+    const uint64_t *q_packed;
+    const int64_t *q_offsets;
+    const int64_t *q_lengths;
+    const uint64_t *r_packed;
+    const int64_t *r_offsets;
+    const int64_t *r_lengths;
+    const int32_t *kinds;    /* per pair 0 = Smith-Waterman, 1 = WFA; NULL: all SW */
+    const int32_t *bands;    /* per pair SW band; NULL: sw_cfg.band_width */
+    gb2_sw_cfg sw_cfg;
+    gb2_wfa_cfg wfa_cfg;
+    gb2_sw_result *sw_out;   /* n_pairs entries; written for SW pairs */
+    int32_t *wfa_out;        /* n_pairs entries; written for WFA pairs */
+} gb2_request;
+
+typedef struct {
+    int64_t hbm_budget_bytes;     /* device bytes admitted requests may hold */
+    int32_t max_inflight_groups;  /* concurrent groups (executors), 1..8 */
+    int32_t max_group_pairs;      /* pairs per group (0: 65536) */
+    int32_t flags;                /* GB2_FLAG_* for the launches */
+} gb2_server_cfg;
+
+typedef struct {
+    int64_t submitted, completed, failed, pairs_completed, groups_launched;
+    int64_t inflight_bytes, peak_inflight_bytes;
+} gb2_server_stats;
+
+typedef struct gb2_server gb2_server;
+
+/* Start a server thread on ctx (which must outlive it). */
+int gb2_server_start(gb2_ctx *ctx, const gb2_server_cfg *cfg, gb2_server **out);
+/* Queue a request; returns at once with a ticket.  GB2_ENOMEM if the request
+   alone can never fit the budget. */
+int gb2_server_submit(gb2_server *srv, const gb2_request *req, uint64_t *ticket);
+/* Non-blocking: *done = 1 once the request's results are in its output arrays. */
+int gb2_server_poll(gb2_server *srv, uint64_t ticket, int *done);
+/* Block until the request is done (GB2_ETIMEOUT after timeout_ms; < 0 waits
+   forever); returns the request's status and its latency from submit to
+   results written.  The ticket is released once reported done. */
+int gb2_server_wait(gb2_server *srv, uint64_t ticket, int timeout_ms, double *latency_ms);
+int gb2_server_stats_get(gb2_server *srv, gb2_server_stats *st);
+/* Finish every queued and running request, then stop the thread. */
+int gb2_server_stop(gb2_server *srv);
+
 /* ---- pinned host memory -----------------------------------------------------------
  * Page-locked host allocations: SequenceBatch arrays built here reach the
  * device by DMA without the library's staging copy. */
@@ -208,7 +276,8 @@ int gb2_flush_l2(gb2_ctx *ctx);
 /* Integer ALU throughput probe: runs dependent-chain microkernels of the
    named instruction class over all SMs and reports giga-ops/s.  kind: 0 IADD,
    1 IMNMX, 2 DPX viaddmax_s32, 3 DPX viaddmax_s16x2, 4 DPX vimax3_s32,
-   5 LOP3, 6 IMAD, 7 SHFL. */
+   5 LOP3, 6 IMAD, 7 SHFL, 8 vimax3_s16x2, 9 vimax3_u16x2, 10 byte_perm,
+   11 viaddmax_s16x2_relu, 12 vimax_s16x2_relu. */
 int gb2_int_peak(gb2_ctx *ctx, int kind, double *gops);
 
 #ifdef __cplusplus

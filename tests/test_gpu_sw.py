@@ -7,7 +7,7 @@ import pytest
 
 import genomics_b200 as G
 from genomics_b200 import AlignConfig, SequenceBatch, synth
-from genomics_b200._lib import FLAG_GENERIC, GenomicsError
+from genomics_b200._lib import FLAG_GENERIC, FLAG_INT32, GenomicsError
 
 pytestmark = pytest.mark.gpu
 
@@ -174,6 +174,26 @@ def test_workload3_mixed_bands(device, oracle):
     assert_same(device.sw_banded(dq, dr, CFG0, bands=bands), ref, "workload 3 resident")
 
 
+@pytest.mark.parametrize("band", [16, 32])
+def test_packed_int16_path_matches_int32_and_oracle(device, oracle, band):
+    """Short pairs (H bound <= 511) take the packed int16x2 kernel by default;
+    GB2_FLAG_INT32 forces the int32 register kernel.  Both equal the oracle."""
+    rng = random.Random(band * 7)
+    q, r = _random_pairs(rng, 3000, 255, "ACGTN")
+    for cfg in (AlignConfig(2, -4, -4, -2, band), AlignConfig(1, -1, 0, -1, band),
+                AlignConfig(3, -2, -6, -1, band), AlignConfig(2, -8, -2, -1, band)):
+        ref = oracle_sw(oracle, q, r, cfg)
+        for batched in (False, True):
+            assert_same(device.sw_banded(q, r, cfg, batched=batched), ref, f"{cfg} packed")
+            assert_same(device.sw_banded(q, r, cfg, batched=batched, flags=FLAG_INT32), ref,
+                        f"{cfg} int32")
+    q, r, _, _ = synth.generate(0, 1000, seed=99)
+    cfg = AlignConfig(2, -4, -4, -2, band)
+    ref = oracle_sw(oracle, q, r, cfg)
+    assert_same(device.sw_banded(q, r, cfg), ref, "reads packed")
+    assert_same(device.sw_banded(q, r, cfg, flags=FLAG_INT32), ref, "reads int32")
+
+
 def test_variants_agree(device, oracle):
     q, r, bands, _ = synth.generate(3, 3000, seed=77)
     ref = oracle_sw(oracle, q, r, CFG0, bands=bands)
@@ -203,3 +223,29 @@ def test_errors(device):
     with pytest.raises(GenomicsError):
         device.sw_banded(dq, dr, CFG0, n_pairs=2)
     assert device.sw_banded(dq, dr, CFG0, n_pairs=0).size == 0
+
+
+def test_device_packing_matches_add_sequence(device, oracle):
+    """gb2_batch_from_ascii packs on the GPU exactly as add_sequence does."""
+    rng = random.Random(31)
+    seqs = ["", "A", "N", "ACGT" * 8, "acgtNNRYacgt", "T" * 33, "G" * 64, "C" * 65]
+    seqs += ["".join(rng.choice("ACGTNacgtn-RYKM") for _ in range(rng.randint(0, 700)))
+             for _ in range(400)]
+    got = device.download_batch(device.batch_from_ascii(seqs))
+    want = SequenceBatch.from_strings(seqs)
+    for x, y in zip(got.arrays(), want.arrays()):
+        assert (x == y).all()
+    for i, s in enumerate(seqs[:60]):
+        op, om = oracle.pack(s)
+        o, nw = int(got.offsets[i]), (len(s) + 31) // 32
+        assert (got.packed[o:o + nw] == op).all() and (got.n_masks[o:o + nw] == om).all()
+    # and a device-packed batch aligns like a host-packed one
+    q, r, bands, _ = synth.generate(3, 500, seed=8)
+    qs = ["".join("ACGT"[(int(w) >> (62 - 2 * j)) & 3] if not (int(m) >> j) & 1 else "N"
+                  for w, m in zip(q.packed[q.offsets[i]:q.offsets[i] + (q.lengths[i] + 31) // 32],
+                                  q.n_masks[q.offsets[i]:q.offsets[i] + (q.lengths[i] + 31) // 32])
+                  for j in range(32))[:q.lengths[i]] for i in range(500)]
+    dq = device.batch_from_ascii(qs)
+    dr = device.upload_batch(r)
+    assert_same(device.sw_banded(dq, dr, CFG0, bands=bands), oracle_sw(oracle, q, r, CFG0, bands=bands),
+                "device-packed queries")
