@@ -223,7 +223,12 @@ __global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *ba
     count_key(counts, key);
 }
 
-__global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int32_t *keys, int *counts)
+// WFA pairs are split into long ones (either sequence at least team_len
+// bases; aligned by a whole block each) and short ones (one warp each), and
+// each class is ordered longest first (length buckets of 16 bases), so the
+// pairs with the longest dependency chains start first.
+__global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int64_t team_len, int32_t *keys,
+                               int *counts)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -232,7 +237,7 @@ __global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int32_t *keys, i
     int64_t lb = l >> 4;
     if (lb > kLenBuckets - 1)
         lb = kLenBuckets - 1;
-    const int key = kLenBuckets - 1 - (int)lb;
+    const int key = (l >= team_len ? 0 : kLenBuckets) + kLenBuckets - 1 - (int)lb;
     keys[i] = key;
     count_key(counts, key);
 }
@@ -506,36 +511,50 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
     const int nslot = hm + 2 * hie;
     const int64_t slot_width = ((qmax + rmax + 5) + 31) & ~int64_t(31);
-    int grid = c->sm_count * 4;
-    if ((int64_t)grid * 4 > n)
-        grid = (int)std::max<int64_t>(1, (n + 3) / 4);
-    const int64_t warps = (int64_t)grid * 4;
+    // blocks of 4 warps, as many per SM as stay resident, fewer when the rings
+    // of that many warps would pass kWfaScratchCap bytes.  Tuning knob in
+    // flags bits 8-15: low 4 bits = blocks per SM, bits 4-5 = kernel unroll
+    // choice, bit 6 = no block-per-pair class, bit 7 = its length threshold 4x.
+    const int variant = (flags >> 8) & 0xff;
+    const int64_t warp_bytes = (int64_t)nslot * slot_width * 4;
+    int64_t grid =
+        (int64_t)c->sm_count * ((variant & 15) ? (variant & 15) : wfa_blocks_per_sm(variant));
+    grid = std::min(grid, std::max<int64_t>(c->sm_count, kWfaScratchCap / (4 * warp_bytes)));
+    grid = std::min(grid, std::max<int64_t>(1, (n + 3) / 4));
     int rc;
-    if ((rc = ensure(c, x.scratch32, (size_t)warps * nslot * slot_width * 4, x.st)) ||
+    if ((rc = ensure(c, x.scratch32, (size_t)(grid * 4 * warp_bytes), x.st)) ||
         (rc = ensure(c, x.counters, kCounterBytes, x.st)))
         return rc;
     CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
-    PairList pl{nullptr, n, nullptr, (int *)x.counters.p};
+    int *const ctr = (int *)x.counters.p;
+    PairList longs{nullptr, 0, nullptr, ctr + kCounterStride};
+    PairList shorts{nullptr, n, nullptr, ctr};
     if (flags & GB2_FLAG_BATCHED) {
-        const int nb = kLenBuckets;
+        const int nb = 2 * kLenBuckets;
+        const int64_t team_len =
+            (variant & 0x40) ? (1ll << 40) : (variant & 0x80 ? 4 : 1) * kWfaTeamMinLen;
         if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
             (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
-            (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) || (rc = ensure(c, x.seg, 16, x.st)))
+            (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) ||
+            (rc = ensure(c, x.seg, 64, x.st)))
             return rc;
         CU(c, cudaMemsetAsync(x.counts.p, 0, (size_t)nb * 4, x.st));
         const int blocks = (int)((n + 255) / 256);
-        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, (int32_t *)x.keys.p,
+        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, team_len, (int32_t *)x.keys.p,
                                                   (int *)x.counts.p);
-        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, nb, (int64_t *)x.seg.p);
+        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, kLenBuckets, (int64_t *)x.seg.p);
         k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
                                              (int32_t *)x.queue.p);
         CU(c, cudaGetLastError());
         c->launches += 3;
-        pl = PairList{(const int32_t *)x.queue.p, 0, (const int64_t *)x.seg.p, (int *)x.counters.p};
+        const int32_t *qd = (const int32_t *)x.queue.p;
+        const int64_t *seg = (const int64_t *)x.seg.p;
+        longs = PairList{qd, 0, seg, ctr + kCounterStride};
+        shorts = PairList{qd, 0, seg + 2, ctr};
     }
     cudaEvent_t e0 = prof_begin(c, x.st);
-    CU(c, launch_wfa(0, qv, rv, p, pl, d_out, (int32_t *)x.scratch32.p, slot_width, grid,
-                     (int *)x.errflag.p, (int64_t *)x.work.p, x.st));
+    CU(c, launch_wfa(variant, qv, rv, p, longs, shorts, d_out, (int32_t *)x.scratch32.p,
+                     slot_width, (int)grid, (int *)x.errflag.p, (int64_t *)x.work.p, x.st));
     prof_end(c, e0, x.st);
     c->launches += 1;
     return GB2_OK;

@@ -86,9 +86,14 @@ struct WfaParams {
     int32_t x, o, e, max_error;
 };
 
-cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList pl, int32_t *out,
-                       int32_t *scratch, int64_t slot_width, int grid, int *err_flag,
-                       int64_t *work, cudaStream_t st);
+// WFA over two pair lists: `longs` one pair per 128-thread block, then
+// `shorts` one pair per warp.  scratch: grid * 4 regions of nslot *
+// slot_width int32.
+// Resident 128-thread blocks per SM of the WFA kernel variant.
+int wfa_blocks_per_sm(int variant);
+cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
+                       PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
+                       int grid, int *err_flag, int64_t *work, cudaStream_t st);
 
 cudaError_t launch_int_peak(int kind, int grid, int block, int iters, uint32_t *sink,
                             cudaStream_t st);

@@ -133,9 +133,10 @@ extern "C" int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
     gb2::SeqView qv{q_packed, q_offsets, q_lengths, 0, q_words};
     gb2::SeqView rv{r_packed, r_offsets, r_lengths, 0, r_words};
     gb2::WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
-    gb2::PairList pl{nullptr, n_pairs, nullptr, counter};
-    if (gb2::launch_wfa(0, qv, rv, p, pl, out_cost, rings, slot_width, (int)blocks, err_flag,
-                        nullptr, st) != cudaSuccess) {
+    const gb2::PairList none{nullptr, 0, nullptr, counter};
+    const gb2::PairList pl{nullptr, n_pairs, nullptr, counter};
+    if (gb2::launch_wfa(0, qv, rv, p, none, pl, out_cost, rings, slot_width, (int)blocks,
+                        err_flag, nullptr, st) != cudaSuccess) {
         cudaGetLastError();
         return GB2_ECUDA;
     }

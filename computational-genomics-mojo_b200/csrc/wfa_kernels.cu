@@ -16,15 +16,14 @@
 //    (M[s-x]; M[s-o-e] +-1; I[s-e] + 1; D[s-e] - 1) intersected with the
 //    reference's [lo, hi] (widened to the target and clamped to +-max_error,
 //    :158-164).  Everything outside it is NEG in the reference.
-//  * NEG is a large negative number and sources are combined with plain max:
-//    a NEG source plus at most one per score stays negative, and every
-//    non-NEG value is >= 0, so "negative" reproduces the reference's
-//    "== NEG_INF" tests (:174-204) and its "row < 0" skip (:211).
+//  * NEG is a large negative number and sources are combined with plain max;
+//    every value below zero is stored as NEG and every non-NEG value is
+//    >= 0, so "negative" reproduces the reference's "== NEG_INF" tests
+//    (:174-204) and its "row < 0" skip (:211).
 //
-// One warp aligns one pair.  Ring slots live in a per-warp scratch region,
-// one int32 per diagonal (index k + rlen + 2).  Invariant: inside the
-// interval [GL, GH] that this pair has touched (every visited interval
-// widened by 2), every slot position outside that slot's own interval holds
+// Ring slots live in a scratch region per warp, one int32 per diagonal
+// (index k + rlen + 2).  Invariant: inside the interval [GL, GH] that a pair
+// has touched, every slot position outside that slot's own interval holds
 // NEG; so source reads at k-1, k, k+1 need no bounds tests.
 #include "gb2_internal.cuh"
 
@@ -42,27 +41,35 @@ __device__ __forceinline__ int gcd_i(int a, int b)
     return a;
 }
 
-// Extend (align_cpu.mojo:208-219), 32 bases per step: XOR of the two
-// unaligned 64-bit windows, count leading zeros, clamp by the remaining
-// lengths (zero padding past a sequence end decodes as A).
-__device__ __forceinline__ int32_t wfa_extend(const SeqView &q, int64_t qoff, int32_t qlen,
-                                              const SeqView &r, int64_t roff, int32_t rlen,
+// 32 bases at position pos of a sequence held in words w[0..last]; w[last]
+// is the word after the sequence's last one (a zero pad in shared memory, or
+// the array's next word in global memory, clamped to the array's end).
+// Bases past the sequence end never matter: matches are clamped by the
+// remaining lengths.
+__device__ __forceinline__ uint64_t window64(const uint64_t *w, int32_t last, int32_t pos)
+{
+    const int32_t i = pos >> 5;
+    const uint32_t sh = (uint32_t)(pos & 31) * 2;
+    const uint64_t a = w[i];
+    const uint64_t b = w[min(i + 1, last)];
+    return (a << sh) | ((b >> 1) >> (63 - sh));
+}
+
+// Extend along diagonal k from row (align_cpu.mojo:208-219): XOR of the two
+// 32-base windows, count leading zeros, clamp by the remaining lengths.
+__device__ __forceinline__ int32_t extend_run(const uint64_t *qw, int32_t qlast, int32_t qlen,
+                                              const uint64_t *rw, int32_t rlast, int32_t rlen,
                                               int32_t row, int32_t k)
 {
-    int32_t col = row - k;
-    if (row < 0 || col < 0)
+    if (row < 0 || row - k < 0)
         return row;
+    int32_t col = row - k;
     while (row < qlen && col < rlen) {
-        const uint64_t a = load_window64(q.packed, q.n_words, qoff, row);
-        const uint64_t b = load_window64(r.packed, r.n_words, roff, col);
-        const uint64_t x = a ^ b;
+        const uint64_t x = window64(qw, qlast, row) ^ window64(rw, rlast, col);
         const int ml = x ? (__clzll((long long)x) >> 1) : 32;
         const int lim = min(qlen - row, rlen - col);
-        if (ml >= lim) {
-            row += lim;
-            col += lim;
-            break;
-        }
+        if (ml >= lim)
+            return row + lim;
         row += ml;
         col += ml;
         if (ml < 32)
@@ -71,242 +78,402 @@ __device__ __forceinline__ int32_t wfa_extend(const SeqView &q, int64_t qoff, in
     return row;
 }
 
-__global__ void __launch_bounds__(128)
-wfa_warp_kernel(SeqView q, SeqView r, WfaParams p, PairList pl, int32_t *__restrict__ out,
-                int32_t *__restrict__ scratch, int64_t slot_width, int *err_flag, int64_t *work)
+// One extend attempt for U diagonals of a thread at once: the first windows
+// of all U are loaded together; a diagonal whose whole window matched goes on
+// in extend_run.
+template <int U>
+__device__ __forceinline__ void extend_u(const uint64_t *qw, int32_t qlast, int32_t qlen,
+                                         const uint64_t *rw, int32_t rlast, int32_t rlen,
+                                         int32_t (&rows)[U], const int32_t (&ks)[U],
+                                         const bool (&live)[U])
 {
-    int64_t n;
-    const int32_t *__restrict__ queue = pairs_resolve(pl, n);
-    int *const queue_counter = pl.counter;
-    const int lane = threadIdx.x & 31;
-    const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
-    const unsigned FULL = 0xffffffffu;
-
-    const int g = gcd_i(p.x, gcd_i(p.o, p.e));
-    const int xs = p.x / g, oes = (p.o + p.e) / g, es = p.e / g;
-    const int hm = max(xs, oes) + 1, hie = es + 1;
-    const int nslot = hm + 2 * hie;
-    int32_t *const region = scratch + warp_global * nslot * slot_width;
-    const int64_t max_err = p.max_error;
-
-    int64_t next = warp_global;
-    for (;;) {
-        int64_t slot_i = next;
-        if (queue_counter) {
-            int64_t b0 = 0;
-            if (lane == 0)
-                b0 = atomicAdd(queue_counter, 1);
-            slot_i = __shfl_sync(FULL, b0, 0);
-        }
-        if (slot_i >= n)
-            break;
-        next += warps_total;
-        const int64_t pi = queue ? (int64_t)queue[slot_i] : slot_i;
-        const int64_t qoff = q.offsets[pi] - q.word_base;
-        const int64_t roff = r.offsets[pi] - r.word_base;
-        const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
-        int32_t result = -1;
-        int64_t cells = 0;
-        if (qlen == 0 && rlen == 0) {
-            result = 0;
-        } else if ((int64_t)qlen + rlen + 5 > slot_width) {
-            if (lane == 0)
-                atomicOr(err_flag, 1);
-            result = -2;
+    uint64_t x[U];
+    int32_t lim[U];
+    bool go[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t col = rows[u] >= 0 ? rows[u] - ks[u] : -1;
+        go[u] = live[u] && rows[u] >= 0 && col >= 0 && rows[u] < qlen && col < rlen;
+        lim[u] = go[u] ? min(qlen - rows[u], rlen - col) : 0;
+        x[u] = 0;
+        if (go[u])
+            x[u] = window64(qw, qlast, rows[u]) ^ window64(rw, rlast, col);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (!go[u])
+            continue;
+        const int ml = x[u] ? (__clzll((long long)x[u]) >> 1) : 32;
+        if (ml >= lim[u]) {
+            rows[u] += lim[u];
         } else {
-            const int32_t kofs = rlen + 2;
-            const int32_t target = qlen - rlen;
-            auto M = [&](int slot) { return region + (int64_t)slot * slot_width + kofs; };
-            auto I = [&](int slot) { return region + (int64_t)(hm + slot) * slot_width + kofs; };
-            auto D = [&](int slot) {
-                return region + (int64_t)(hm + hie + slot) * slot_width + kofs;
-            };
-            // per-slot intervals: lane j holds slot j's (ring sizes <= 32)
-            int32_t mlo = 1, mhi = 0, ilo = 1, ihi = 0, dlo = 1, dhi = 0;
-            int32_t GL = max(-2, -rlen - 2), GH = min(2, qlen + 2);
-            for (int sl = 0; sl < nslot; ++sl) {
-                int32_t *row = region + (int64_t)sl * slot_width + kofs;
-                for (int32_t k = GL + lane; k <= GH; k += 32)
-                    row[k] = WFA_NEG;
-            }
-            __syncwarp();
-            // score 0: M[0,0] = 0 extended along diagonal 0 (:130-140)
-            int32_t row0 = 0;
-            if (lane == 0) {
-                row0 = wfa_extend(q, qoff, qlen, r, roff, rlen, 0, 0);
-                M(0)[0] = row0;
-            }
-            row0 = __shfl_sync(FULL, row0, 0);
-            if (lane == 0) {
-                mlo = 0;
-                mhi = 0;
-            }
-            __syncwarp();
-            if (target == 0 && row0 >= qlen && max_err >= 0) {
-                result = 0;
-            } else {
-                for (int64_t sp = 1; sp * g <= max_err; ++sp) {
-                    const int64_t s = sp * g;
-                    int64_t lo = max((int64_t)-rlen, -s), hi = min((int64_t)qlen, s);
-                    if (target < lo || target > hi) {
-                        lo = min(lo, (int64_t)target);
-                        hi = max(hi, (int64_t)target);
-                    }
-                    lo = max(lo, -max_err);
-                    hi = min(hi, max_err);
-                    int32_t ulo = 0x7fffffff, uhi = -0x7fffffff;
-                    const int sx = sp >= xs ? (int)((sp - xs) % hm) : -1;
-                    const int soe = sp >= oes ? (int)((sp - oes) % hm) : -1;
-                    const int se = sp >= es ? (int)((sp - es) % hie) : -1;
-                    if (sx >= 0) {
-                        const int32_t a0 = __shfl_sync(FULL, mlo, sx), b0 = __shfl_sync(FULL, mhi, sx);
-                        if (a0 <= b0) {
-                            ulo = min(ulo, a0);
-                            uhi = max(uhi, b0);
-                        }
-                    }
-                    if (soe >= 0) {
-                        const int32_t a0 = __shfl_sync(FULL, mlo, soe), b0 = __shfl_sync(FULL, mhi, soe);
-                        if (a0 <= b0) {
-                            ulo = min(ulo, a0 - 1);
-                            uhi = max(uhi, b0 + 1);
-                        }
-                    }
-                    if (se >= 0) {
-                        const int32_t a0 = __shfl_sync(FULL, ilo, se), b0 = __shfl_sync(FULL, ihi, se);
-                        if (a0 <= b0) {
-                            ulo = min(ulo, a0 + 1);
-                            uhi = max(uhi, b0 + 1);
-                        }
-                        const int32_t a1 = __shfl_sync(FULL, dlo, se), b1 = __shfl_sync(FULL, dhi, se);
-                        if (a1 <= b1) {
-                            ulo = min(ulo, a1 - 1);
-                            uhi = max(uhi, b1 - 1);
-                        }
-                    }
-                    const int32_t a = (int32_t)max((int64_t)ulo, lo);
-                    const int32_t b = (int32_t)min((int64_t)uhi, hi);
-                    const int ms = (int)(sp % hm), is = (int)(sp % hie);
-                    const int32_t omlo = __shfl_sync(FULL, mlo, ms), omhi = __shfl_sync(FULL, mhi, ms);
-                    const int32_t oilo = __shfl_sync(FULL, ilo, is), oihi = __shfl_sync(FULL, ihi, is);
-                    const int32_t odlo = __shfl_sync(FULL, dlo, is), odhi = __shfl_sync(FULL, dhi, is);
-                    int32_t *Mw = M(ms), *Iw = I(is), *Dw = D(is);
-                    if (a > b) {
-                        // empty score: clear what the reused slots held
-                        for (int32_t k = omlo + lane; k <= omhi; k += 32)
-                            Mw[k] = WFA_NEG;
-                        for (int32_t k = oilo + lane; k <= oihi; k += 32)
-                            Iw[k] = WFA_NEG;
-                        for (int32_t k = odlo + lane; k <= odhi; k += 32)
-                            Dw[k] = WFA_NEG;
-                        if (lane == ms) {
-                            mlo = 1;
-                            mhi = 0;
-                        }
-                        if (lane == is) {
-                            ilo = dlo = 1;
-                            ihi = dhi = 0;
-                        }
-                        __syncwarp();
-                        continue;
-                    }
-                    cells += (int64_t)(b - a + 1);
-                    // widen the touched interval to [a-2, b+2]
-                    const int32_t nGL = max(min(GL, a - 2), -rlen - 2);
-                    const int32_t nGH = min(max(GH, b + 2), qlen + 2);
-                    if (nGL < GL || nGH > GH) {
-                        for (int sl = 0; sl < nslot; ++sl) {
-                            int32_t *rowp = region + (int64_t)sl * slot_width + kofs;
-                            for (int32_t k = nGL + lane; k < GL; k += 32)
-                                rowp[k] = WFA_NEG;
-                            for (int32_t k = GH + 1 + lane; k <= nGH; k += 32)
-                                rowp[k] = WFA_NEG;
-                        }
-                        GL = nGL;
-                        GH = nGH;
-                        __syncwarp();
-                    }
-                    const int32_t *Mx = sx >= 0 ? M(sx) : nullptr;
-                    const int32_t *Moe = soe >= 0 ? M(soe) : nullptr;
-                    const int32_t *Ie = se >= 0 ? I(se) : nullptr;
-                    const int32_t *De = se >= 0 ? D(se) : nullptr;
-                    for (int32_t k = a + lane; k <= b; k += 32) {
-                        int32_t iv = WFA_NEG, dv = WFA_NEG, mv = WFA_NEG;
-                        if (Moe) {
-                            iv = Moe[k - 1];
-                            dv = Moe[k + 1];
-                        }
-                        if (Ie) {
-                            iv = max(iv, Ie[k - 1]);
-                            dv = max(dv, De[k + 1]);
-                        }
-                        iv += 1;
-                        if (Mx)
-                            mv = Mx[k] + 1;
-                        mv = max(mv, max(iv, dv));
-                        Iw[k] = iv;
-                        Dw[k] = dv;
-                        Mw[k] = mv;
-                    }
-                    // old contents of the reused slots outside [a, b] -> NEG
-                    for (int32_t k = omlo + lane; k <= omhi; k += 32)
-                        if (k < a || k > b)
-                            Mw[k] = WFA_NEG;
-                    for (int32_t k = oilo + lane; k <= oihi; k += 32)
-                        if (k < a || k > b)
-                            Iw[k] = WFA_NEG;
-                    for (int32_t k = odlo + lane; k <= odhi; k += 32)
-                        if (k < a || k > b)
-                            Dw[k] = WFA_NEG;
-                    if (lane == ms) {
-                        mlo = a;
-                        mhi = b;
-                    }
-                    if (lane == is) {
-                        ilo = dlo = a;
-                        ihi = dhi = b;
-                    }
-                    // extend this lane's diagonals (the lane wrote them itself)
-                    for (int32_t k = a + lane; k <= b; k += 32) {
-                        const int32_t row = Mw[k];
-                        if (row >= 0)
-                            Mw[k] = wfa_extend(q, qoff, qlen, r, roff, rlen, row, k);
-                    }
-                    bool done = false;
-                    if (target >= lo && target <= hi && target >= a && target <= b) {
-                        const int owner = (target - a) & 31;
-                        int32_t v = 0;
-                        if (lane == owner)
-                            v = Mw[target];
-                        v = __shfl_sync(FULL, v, owner);
-                        done = v >= qlen;
-                    }
-                    __syncwarp();
-                    if (done) {
-                        result = (int32_t)s;
-                        break;
-                    }
-                }
-            }
-        }
-        if (lane == 0) {
-            out[pi] = result;
-            if (work)
-                atomicAdd((unsigned long long *)work, (unsigned long long)cells);
+            rows[u] += ml;
+            if (ml == 32)
+                rows[u] = extend_run(qw, qlast, qlen, rw, rlast, rlen, rows[u], ks[u]);
         }
     }
 }
 
-cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList pl, int32_t *out,
-                       int32_t *scratch, int64_t slot_width, int grid, int *err_flag,
-                       int64_t *work, cudaStream_t st)
+// Pair alignment by a team of TEAM warps (TEAM = 1: one warp; TEAM = 4: the
+// whole 128-thread block).  Thread tt of the team owns diagonals
+// a + tt + 32*TEAM*j of the visited interval.  Per score step:
+//  * ring slots advance by one (no division);
+//  * every warp keeps its own copy of the per-slot intervals (lane j holds
+//    slot j's) and computes the same [a, b];
+//  * the reused destination slots are cleaned only where their old interval
+//    pokes out of [a, b];
+//  * each thread loads the sources of U diagonals together (they live in
+//    other slots than the ones written, so nothing written in the step is
+//    read back in it), computes, extends and stores each diagonal once;
+//    values below zero are stored as NEG, so NEG never drifts;
+//  * the touched interval [GL, GH] is widened at the END of the step, with
+//    kWfaWiden spare diagonals, so that it holds [a-2, b+2].  The next
+//    step's interval reaches at most one diagonal past every earlier one and
+//    reads one more on each side, so its reads stay inside what earlier
+//    steps filled, and a step needs one team barrier (which also ORs the
+//    "target reached" flags).
+// Both sequences are copied into shared memory when each fits seqw - 1
+// words; longer ones are read from global memory.
+constexpr int kWfaSeqWords = 321;  // per sequence per warp: 10,240 bases + a zero pad
+constexpr int kWfaWiden = 30;
+constexpr int kWfaTeamSeqWords = 4 * kWfaSeqWords;  // team mode: 41,056 bases + pad
+
+// Team barrier with memory ordering that also ORs a flag over the team.
+template <int TEAM>
+__device__ __forceinline__ bool team_any(bool v)
 {
-    (void)variant;
-    if (!pl.seg && pl.n <= 0)
-        return cudaSuccess;
-    wfa_warp_kernel<<<grid, 128, 0, st>>>(q, r, p, pl, out, scratch, slot_width, err_flag,
-                                          work);
+    if (TEAM == 1) {
+        __syncwarp();
+        return __any_sync(0xffffffffu, v);
+    }
+    return __syncthreads_or(v) != 0;
+}
+
+template <int TEAM>
+__device__ __forceinline__ void team_sync()
+{
+    if (TEAM == 1)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+struct WfaShape {
+    int g, xs, oes, es, hm, hie, nslot;
+};
+
+template <int U, int TEAM>
+__device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &r,
+                                               const WfaParams &p, const WfaShape &w,
+                                               int64_t pi, int32_t *region, int64_t slot_width,
+                                               uint64_t *sq, uint64_t *sr, int seqw,
+                                               int32_t *__restrict__ out, int *err_flag,
+                                               int64_t *work)
+{
+    constexpr int TW = TEAM * 32;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int tt = TEAM == 1 ? lane : (int)threadIdx.x;
+    const int hm = w.hm, hie = w.hie, xs = w.xs, oes = w.oes, es = w.es, g = w.g;
+    const int32_t max_err = p.max_error;
+    const int64_t qoff = q.offsets[pi] - q.word_base;
+    const int64_t roff = r.offsets[pi] - r.word_base;
+    const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
+    int32_t result = -1;
+    int64_t cells = 0;
+    if (qlen == 0 && rlen == 0) {
+        result = 0;
+    } else if ((int64_t)qlen + rlen + 5 > slot_width) {
+        if (tt == 0)
+            atomicOr(err_flag, 1);
+        result = -2;
+    } else {
+        const int32_t qnw = (qlen + 31) >> 5, rnw = (rlen + 31) >> 5;
+        const uint64_t *qw, *rw;
+        int32_t qlast, rlast;
+        team_sync<TEAM>();  // the previous pair's reads of the shared copies are done
+        if (qnw < seqw) {
+            for (int i = tt; i <= qnw; i += TW)
+                sq[i] = i < qnw ? __ldg(q.packed + qoff + i) : 0;
+            qw = sq;
+            qlast = qnw;
+        } else {
+            qw = q.packed + qoff;
+            qlast = (int32_t)min(q.n_words - 1 - qoff, (int64_t)0x7fffffff);
+        }
+        if (rnw < seqw) {
+            for (int i = tt; i <= rnw; i += TW)
+                sr[i] = i < rnw ? __ldg(r.packed + roff + i) : 0;
+            rw = sr;
+            rlast = rnw;
+        } else {
+            rw = r.packed + roff;
+            rlast = (int32_t)min(r.n_words - 1 - roff, (int64_t)0x7fffffff);
+        }
+        const int32_t kofs = rlen + 2;
+        const int32_t target = qlen - rlen;
+        int32_t *const base = region + kofs;
+        auto M = [&](int slot) { return base + (int64_t)slot * slot_width; };
+        auto I = [&](int slot) { return base + (int64_t)(hm + slot) * slot_width; };
+        auto D = [&](int slot) { return base + (int64_t)(hm + hie + slot) * slot_width; };
+        // per-slot intervals: lane j holds M slot j's and I/D slot j's (I and
+        // D of one score always share their interval; ring sizes <= 32)
+        int32_t mlo = 1, mhi = 0, ilo = 1, ihi = 0;
+        int32_t GL = max(-2, -rlen - 2), GH = min(2, qlen + 2);
+        for (int sl = 0; sl < w.nslot; ++sl) {
+            int32_t *row = base + (int64_t)sl * slot_width;
+            for (int32_t k = GL + tt; k <= GH; k += TW)
+                row[k] = WFA_NEG;
+        }
+        team_sync<TEAM>();
+        // score 0: M[0,0] = 0 extended along diagonal 0 (:130-140); every
+        // thread computes it, thread 0 stores it
+        const int32_t row0 = extend_run(qw, qlast, qlen, rw, rlast, rlen, 0, 0);
+        if (lane == 0) {
+            mlo = 0;
+            mhi = 0;
+        }
+        if (tt == 0)
+            M(0)[0] = row0;
+        team_sync<TEAM>();
+        if (target == 0 && row0 >= qlen) {
+            result = 0;
+        } else {
+            int ms = 0, is = 0;  // ring slots of the current score
+            for (int64_t sp = 1; sp * g <= max_err; ++sp) {
+                const int32_t s = (int32_t)(sp * g);
+                ms = ms + 1 == hm ? 0 : ms + 1;
+                is = is + 1 == hie ? 0 : is + 1;
+                int32_t lo = max(-rlen, -s), hi = min(qlen, s);
+                if (target < lo || target > hi) {
+                    lo = min(lo, target);
+                    hi = max(hi, target);
+                }
+                lo = max(lo, -max_err);
+                hi = min(hi, max_err);
+                const int sx = sp >= xs ? (ms >= xs ? ms - xs : ms - xs + hm) : -1;
+                const int soe = sp >= oes ? (ms >= oes ? ms - oes : ms - oes + hm) : -1;
+                const int se = sp >= es ? (is >= es ? is - es : is - es + hie) : -1;
+                int32_t ulo = 0x7fffffff, uhi = -0x7fffffff;
+                {
+                    const int32_t a0 = __shfl_sync(FULL, mlo, sx & 31);
+                    const int32_t b0 = __shfl_sync(FULL, mhi, sx & 31);
+                    if (sx >= 0 && a0 <= b0) {
+                        ulo = a0;
+                        uhi = b0;
+                    }
+                    const int32_t a1 = __shfl_sync(FULL, mlo, soe & 31);
+                    const int32_t b1 = __shfl_sync(FULL, mhi, soe & 31);
+                    if (soe >= 0 && a1 <= b1) {
+                        ulo = min(ulo, a1 - 1);
+                        uhi = max(uhi, b1 + 1);
+                    }
+                    const int32_t a2 = __shfl_sync(FULL, ilo, se & 31);
+                    const int32_t b2 = __shfl_sync(FULL, ihi, se & 31);
+                    if (se >= 0 && a2 <= b2) {  // I[s-e] at k-1 and D[s-e] at k+1
+                        ulo = min(ulo, a2 - 1);
+                        uhi = max(uhi, b2 + 1);
+                    }
+                }
+                const int32_t a = max(ulo, lo);
+                const int32_t b = min(uhi, hi);
+                const int32_t omlo = __shfl_sync(FULL, mlo, ms);
+                const int32_t omhi = __shfl_sync(FULL, mhi, ms);
+                const int32_t oilo = __shfl_sync(FULL, ilo, is);
+                const int32_t oihi = __shfl_sync(FULL, ihi, is);
+                int32_t *const Mw = M(ms), *const Iw = I(is), *const Dw = D(is);
+                // what the reused slots held outside [a, b] becomes NEG (all
+                // of it when this score is empty)
+                const int32_t ca = a > b ? 0x7fffffff : a, cb = a > b ? -0x7fffffff : b;
+                if ((omlo <= omhi && (omlo < ca || omhi > cb)) ||
+                    (oilo <= oihi && (oilo < ca || oihi > cb))) {
+                    for (int32_t k = omlo + tt; k <= min(omhi, ca - 1); k += TW)
+                        Mw[k] = WFA_NEG;
+                    for (int32_t k = max(omlo, cb + 1) + tt; k <= omhi; k += TW)
+                        Mw[k] = WFA_NEG;
+                    for (int32_t k = oilo + tt; k <= min(oihi, ca - 1); k += TW) {
+                        Iw[k] = WFA_NEG;
+                        Dw[k] = WFA_NEG;
+                    }
+                    for (int32_t k = max(oilo, cb + 1) + tt; k <= oihi; k += TW) {
+                        Iw[k] = WFA_NEG;
+                        Dw[k] = WFA_NEG;
+                    }
+                }
+                bool hit = false;
+                if (a <= b) {
+                    cells += (int64_t)(b - a + 1);
+                    const int32_t *Mx = sx >= 0 ? M(sx) : nullptr;
+                    const int32_t *Moe = soe >= 0 ? M(soe) : nullptr;
+                    const int32_t *Ie = se >= 0 ? I(se) : nullptr;
+                    const int32_t *De = se >= 0 ? D(se) : nullptr;
+                    for (int32_t k0 = a + tt; k0 <= b; k0 += TW * U) {
+                        int32_t ks[U], iv[U], dv[U], mv[U];
+                        bool live[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            ks[u] = k0 + TW * u;
+                            live[u] = ks[u] <= b;
+                            const int32_t kc = live[u] ? ks[u] : b;  // loads stay in [a-1, b+1]
+                            int32_t i0 = WFA_NEG, d0 = WFA_NEG, m0 = WFA_NEG;
+                            if (Moe) {
+                                i0 = Moe[kc - 1];
+                                d0 = Moe[kc + 1];
+                            }
+                            if (Ie) {
+                                i0 = max(i0, Ie[kc - 1]);
+                                d0 = max(d0, De[kc + 1]);
+                            }
+                            if (Mx)
+                                m0 = Mx[kc] + 1;
+                            iv[u] = i0 < 0 ? WFA_NEG : i0 + 1;
+                            dv[u] = d0;
+                            const int32_t m1 = max(m0, max(iv[u], d0));
+                            mv[u] = m1 < 0 ? WFA_NEG : m1;
+                        }
+                        extend_u<U>(qw, qlast, qlen, rw, rlast, rlen, mv, ks, live);
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (live[u]) {
+                                Iw[ks[u]] = iv[u];
+                                Dw[ks[u]] = dv[u];
+                                Mw[ks[u]] = mv[u];
+                                hit |= ks[u] == target && mv[u] >= qlen;
+                            }
+                        }
+                    }
+                    // widen for the next step (see above); the positions
+                    // filled lie outside everything this step reads or writes
+                    if (a - 2 < GL || b + 2 > GH) {
+                        const int32_t nGL = a - 2 < GL ? max(a - 2 - kWfaWiden, -rlen - 2) : GL;
+                        const int32_t nGH = b + 2 > GH ? min(b + 2 + kWfaWiden, qlen + 2) : GH;
+                        for (int sl = 0; sl < w.nslot; ++sl) {
+                            int32_t *rowp = base + (int64_t)sl * slot_width;
+                            for (int32_t k = nGL + tt; k < GL; k += TW)
+                                rowp[k] = WFA_NEG;
+                            for (int32_t k = GH + 1 + tt; k <= nGH; k += TW)
+                                rowp[k] = WFA_NEG;
+                        }
+                        GL = nGL;
+                        GH = nGH;
+                    }
+                }
+                if (lane == ms) {
+                    mlo = a <= b ? a : 1;
+                    mhi = a <= b ? b : 0;
+                }
+                if (lane == is) {
+                    ilo = a <= b ? a : 1;
+                    ihi = a <= b ? b : 0;
+                }
+                // M[s, target] >= qlen ends the alignment (:221-224); target
+                // inside [a, b] is inside the reference's [lo, hi]
+                if (team_any<TEAM>(hit)) {
+                    result = s;
+                    break;
+                }
+            }
+        }
+    }
+    if (tt == 0) {
+        out[pi] = result;
+        if (work)
+            atomicAdd((unsigned long long *)work, (unsigned long long)cells);
+    }
+}
+
+// Persistent kernel over two length-sorted queues: every block first takes
+// pairs of `longs` one at a time as a team of its 4 warps (a long pair's
+// score steps are its critical path, so four warps share each step); when
+// that queue is empty each warp takes pairs of `shorts` on its own.  Ring
+// slots: one region of nslot * slot_width int32 per warp (team mode uses the
+// block's first).
+template <int U>
+__global__ void __launch_bounds__(128)
+wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
+           int32_t *__restrict__ out, int32_t *__restrict__ scratch, int64_t slot_width,
+           int *err_flag, int64_t *work)
+{
+    __shared__ uint64_t seqs[4 * 2 * kWfaSeqWords];
+    __shared__ int64_t team_slot;
+    WfaShape w;
+    w.g = gcd_i(p.x, gcd_i(p.o, p.e));
+    w.xs = p.x / w.g;
+    w.oes = (p.o + p.e) / w.g;
+    w.es = p.e / w.g;
+    w.hm = max(w.xs, w.oes) + 1;
+    w.hie = w.es + 1;
+    w.nslot = w.hm + 2 * w.hie;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t region_words = (int64_t)w.nslot * slot_width;
+
+    int64_t nl;
+    const int32_t *__restrict__ lq = pairs_resolve(longs, nl);
+    if (nl > 0) {
+        int32_t *const region = scratch + (int64_t)blockIdx.x * 4 * region_words;
+        for (;;) {
+            __syncthreads();
+            if (threadIdx.x == 0)
+                team_slot = atomicAdd(longs.counter, 1);
+            __syncthreads();
+            const int64_t si = team_slot;
+            if (si >= nl)
+                break;
+            const int64_t pi = lq ? (int64_t)lq[si] : si;
+            wfa_align_pair<U, 4>(q, r, p, w, pi, region, slot_width, seqs,
+                                 seqs + kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag, work);
+        }
+        __syncthreads();  // shared copies of the last long pair are no longer read
+    }
+
+    int64_t ns;
+    const int32_t *__restrict__ sq = pairs_resolve(shorts, ns);
+    int32_t *const region = scratch + ((int64_t)blockIdx.x * 4 + wib) * region_words;
+    uint64_t *const my = seqs + (int64_t)wib * 2 * kWfaSeqWords;
+    for (;;) {
+        int64_t b0 = 0;
+        if (lane == 0)
+            b0 = atomicAdd(shorts.counter, 1);
+        const int64_t si = __shfl_sync(0xffffffffu, b0, 0);
+        if (si >= ns)
+            break;
+        const int64_t pi = sq ? (int64_t)sq[si] : si;
+        wfa_align_pair<U, 1>(q, r, p, w, pi, region, slot_width, my, my + kWfaSeqWords,
+                             kWfaSeqWords, out, err_flag, work);
+    }
+}
+
+int wfa_blocks_per_sm(int variant)
+{
+    int n = 0;
+    cudaError_t e;
+    if (variant & 0x20)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<1>, 128, 0);
+    else if (variant & 0x10)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<2>, 128, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<4>, 128, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 4;
+    }
+    return n > 0 ? n : 1;
+}
+
+cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
+                       PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
+                       int grid, int *err_flag, int64_t *work, cudaStream_t st)
+{
+    // variant bits 4-5: diagonals per thread per round 4 (default), 2 or 1
+    if (variant & 0x20)
+        wfa_kernel<1><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
+                                            err_flag, work);
+    else if (variant & 0x10)
+        wfa_kernel<2><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
+                                            err_flag, work);
+    else
+        wfa_kernel<4><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
+                                            err_flag, work);
     return cudaGetLastError();
 }
 

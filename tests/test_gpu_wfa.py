@@ -111,3 +111,70 @@ def test_errors(device):
                 WFAConfig(4, 6, 2, -1), WFAConfig(100, 6, 1, 10)):
         with pytest.raises(GenomicsError):
             device.wfa_affine(q, r, bad)
+
+
+def _random_seq(rng, n):
+    return "".join(rng.choice("ACGT") for _ in range(n))
+
+
+def _mutate(rng, q, rate):
+    r = list(q)
+    for _k in range(int(len(q) * rate)):
+        pos = rng.randint(0, max(len(r) - 1, 0))
+        op = rng.random()
+        if op < 0.6 and r:
+            r[pos] = rng.choice("ACGT")
+        elif op < 0.8:
+            r[pos:pos] = rng.choice("ACGT") * rng.randint(1, 4)
+        elif r:
+            del r[pos:pos + rng.randint(1, 4)]
+    return "".join(r)
+
+
+def test_length_classes(device, oracle):
+    """Pairs on both sides of the block-per-pair threshold (2,048 bases), of
+    the per-warp and per-block shared-memory sequence copies (10,240 and
+    41,056 bases), unrelated pairs whose diagonal interval grows to thousands,
+    and long pairs: batched, plain and tuning variants against the oracle."""
+    rng = random.Random(2024)
+    qs, rs = [], []
+    for _ in range(40):                       # around the threshold, narrow intervals
+        q = _random_seq(rng, rng.randint(1500, 3072))
+        qs.append(q)
+        rs.append(_mutate(rng, q, 0.05))
+    for _ in range(6):                        # unrelated: interval > 1024
+        qs.append(_random_seq(rng, rng.randint(2500, 3072)))
+        rs.append(_random_seq(rng, rng.randint(2500, 3072)))
+    for _ in range(12):                       # past the per-warp shared copies
+        q = _random_seq(rng, rng.randint(3073, 20480))
+        qs.append(q)
+        rs.append(_mutate(rng, q, 0.03)[:20480])
+    for _ in range(3):                        # unrelated: interval > 8192
+        qs.append(_random_seq(rng, rng.randint(9000, 10000)))
+        rs.append(_random_seq(rng, rng.randint(9000, 10000)))
+    for _ in range(3):                        # long
+        q = _random_seq(rng, rng.randint(20481, 24000))
+        qs.append(q)
+        rs.append(_mutate(rng, q, 0.02))
+    for _ in range(2):                        # too long for a block's shared copies
+        q = _random_seq(rng, rng.randint(41100, 45000))
+        qs.append(q)
+        rs.append(_mutate(rng, q, 0.01))
+    order = list(range(len(qs)))
+    rng.shuffle(order)
+    q = SequenceBatch.from_strings([qs[i] for i in order])
+    r = SequenceBatch.from_strings([rs[i] for i in order])
+    for me in (3000, 24000):
+        cfg = WFAConfig(4, 6, 2, me)
+        ref = oracle_wfa(oracle, q, r, cfg)
+        assert (ref >= 0).any()
+        assert_same(device.wfa_affine(q, r, cfg, batched=True), ref, f"classes me={me}")
+        assert_same(device.wfa_affine(q, r, cfg, batched=False), ref, f"plain me={me}")
+        # every pair one warp each (no block-per-pair class), and a 4x threshold
+        for v in (0x40, 0x80):
+            assert_same(device.wfa_affine(q, r, cfg, batched=True, flags=v << 8), ref,
+                        f"variant {v:#x} me={me}")
+    # penalties with gcd 1 and 14 ring slots
+    cfg = WFAConfig(5, 2, 3, 3000)
+    ref = oracle_wfa(oracle, q, r, cfg)
+    assert_same(device.wfa_affine(q, r, cfg, batched=True), ref, "(5,2,3)")
