@@ -223,12 +223,10 @@ __global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *ba
     count_key(counts, key);
 }
 
-// WFA pairs are split into long ones (either sequence at least team_len
-// bases; aligned by a whole block each) and short ones (one warp each), and
-// each class is ordered longest first (length buckets of 16 bases), so the
-// pairs with the longest dependency chains start first.
-__global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int64_t team_len, int32_t *keys,
-                               int *counts)
+// WFA pairs are ordered longest first (length buckets of 16 bases, the
+// longer of the two sequences), so the pairs with the longest dependency
+// chains start first.
+__global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int32_t *keys, int *counts)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -237,9 +235,26 @@ __global__ void k_classify_wfa(int64_t n, SeqView q, SeqView r, int64_t team_len
     int64_t lb = l >> 4;
     if (lb > kLenBuckets - 1)
         lb = kLenBuckets - 1;
-    const int key = (l >= team_len ? 0 : kLenBuckets) + kLenBuckets - 1 - (int)lb;
+    const int key = kLenBuckets - 1 - (int)lb;
     keys[i] = key;
     count_key(counts, key);
+}
+
+// Splits the longest-first WFA queue after its scan: the first
+// min(team_pairs, pairs at least team_len long) pairs are aligned by a whole
+// block each, the rest by one warp each.  seg = {0, split, split, n}.
+__global__ void k_split_wfa(const int *starts, int64_t n, int64_t team_len, int64_t team_pairs,
+                            int64_t *seg)
+{
+    const int64_t lb = team_len >> 4;
+    int64_t longs = lb > kLenBuckets - 1 ? 0 : starts[kLenBuckets - (int)lb];
+    if (lb <= 0)
+        longs = n;
+    const int64_t split = longs < team_pairs ? longs : team_pairs;
+    seg[0] = 0;
+    seg[1] = split;
+    seg[2] = split;
+    seg[3] = n;
 }
 
 // Exclusive scan of counts[nb] (one block); writes cursors into counts and
@@ -514,7 +529,8 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     // blocks of 4 warps, as many per SM as stay resident, fewer when the rings
     // of that many warps would pass kWfaScratchCap bytes.  Tuning knob in
     // flags bits 8-15: low 4 bits = blocks per SM, bits 4-5 = kernel unroll
-    // choice, bit 6 = no block-per-pair class, bit 7 = its length threshold 4x.
+    // choice, bit 6 = no pair aligned by a whole block, bit 7 = every pair of
+    // at least kWfaTeamMinLen bases aligned by a whole block.
     const int variant = (flags >> 8) & 0xff;
     const int64_t warp_bytes = (int64_t)nslot * slot_width * 4;
     int64_t grid =
@@ -530,9 +546,9 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     PairList longs{nullptr, 0, nullptr, ctr + kCounterStride};
     PairList shorts{nullptr, n, nullptr, ctr};
     if (flags & GB2_FLAG_BATCHED) {
-        const int nb = 2 * kLenBuckets;
-        const int64_t team_len =
-            (variant & 0x40) ? (1ll << 40) : (variant & 0x80 ? 4 : 1) * kWfaTeamMinLen;
+        const int nb = kLenBuckets;
+        // one pair per block for the longest pairs, one wave of blocks of them
+        const int64_t team_pairs = (variant & 0x40) ? 0 : (variant & 0x80) ? n : grid;
         if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
             (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
             (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) ||
@@ -540,15 +556,17 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
             return rc;
         CU(c, cudaMemsetAsync(x.counts.p, 0, (size_t)nb * 4, x.st));
         const int blocks = (int)((n + 255) / 256);
-        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, team_len, (int32_t *)x.keys.p,
+        int64_t *seg = (int64_t *)x.seg.p;
+        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, (int32_t *)x.keys.p,
                                                   (int *)x.counts.p);
-        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, kLenBuckets, (int64_t *)x.seg.p);
+        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, nb, seg);
+        k_split_wfa<<<1, 1, 0, x.st>>>((const int *)x.counts.p, n, kWfaTeamMinLen, team_pairs,
+                                       seg);
         k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
                                              (int32_t *)x.queue.p);
         CU(c, cudaGetLastError());
-        c->launches += 3;
+        c->launches += 4;
         const int32_t *qd = (const int32_t *)x.queue.p;
-        const int64_t *seg = (const int64_t *)x.seg.p;
         longs = PairList{qd, 0, seg, ctr + kCounterStride};
         shorts = PairList{qd, 0, seg + 2, ctr};
     }

@@ -16,7 +16,7 @@ constexpr int kLenBuckets = 1024;  // length buckets per class
 constexpr int64_t kPinChunk = 32ll << 20;
 constexpr int64_t kPackHmax = 511;  // packed kernel: H*128 + column fits 16 bits
 constexpr int64_t kWfaScratchCap = 8ll << 30;  // WFA rings of all warps, bytes
-constexpr int64_t kWfaTeamMinLen = 2048;       // WFA pairs this long: one block each
+constexpr int64_t kWfaTeamMinLen = 2048;       // shortest WFA pair aligned by a whole block
 
 // Grow-only device buffer.
 struct DevBuf {

@@ -41,38 +41,46 @@ __device__ __forceinline__ int gcd_i(int a, int b)
     return a;
 }
 
-// 32 bases at position pos of a sequence held in words w[0..last]; w[last]
-// is the word after the sequence's last one (a zero pad in shared memory, or
-// the array's next word in global memory, clamped to the array's end).
-// Bases past the sequence end never matter: matches are clamped by the
-// remaining lengths.
-__device__ __forceinline__ uint64_t window64(const uint64_t *w, int32_t last, int32_t pos)
+// A sequence as 32-bit halves of its packed words (16 bases each, MSB
+// first): logical half j sits at w[j ^ swz] -- swz = 0 for the shared-memory
+// copy (stored high half first), 1 for the packed words in global memory
+// (little-endian, so a word's high half comes second).  Logical half `last`
+// is the one after the sequence's last half (a zero pad in shared memory, or
+// the array's next half in global memory, clamped to the array's end).
+struct SeqHalves {
+    const uint32_t *w;
+    int32_t last;
+    uint32_t swz;
+};
+
+// 16 bases at position pos: one funnel shift of two halves.  Bases past the
+// sequence end never matter: matches are clamped by the remaining lengths.
+__device__ __forceinline__ uint32_t window16(const SeqHalves &s, int32_t pos)
 {
-    const int32_t i = pos >> 5;
-    const uint32_t sh = (uint32_t)(pos & 31) * 2;
-    const uint64_t a = w[i];
-    const uint64_t b = w[min(i + 1, last)];
-    return (a << sh) | ((b >> 1) >> (63 - sh));
+    const int32_t j = pos >> 4;
+    const uint32_t hi = s.w[(uint32_t)j ^ s.swz];
+    const uint32_t lo = s.w[(uint32_t)min(j + 1, s.last) ^ s.swz];
+    return __funnelshift_l(lo, hi, (uint32_t)(pos & 15) << 1);
 }
 
 // Extend along diagonal k from row (align_cpu.mojo:208-219): XOR of the two
-// 32-base windows, count leading zeros, clamp by the remaining lengths.
-__device__ __forceinline__ int32_t extend_run(const uint64_t *qw, int32_t qlast, int32_t qlen,
-                                              const uint64_t *rw, int32_t rlast, int32_t rlen,
-                                              int32_t row, int32_t k)
+// 16-base windows, count leading zeros, clamp by the remaining lengths.
+__device__ __forceinline__ int32_t extend_run(const SeqHalves &qs, int32_t qlen,
+                                              const SeqHalves &rs, int32_t rlen, int32_t row,
+                                              int32_t k)
 {
     if (row < 0 || row - k < 0)
         return row;
     int32_t col = row - k;
     while (row < qlen && col < rlen) {
-        const uint64_t x = window64(qw, qlast, row) ^ window64(rw, rlast, col);
-        const int ml = x ? (__clzll((long long)x) >> 1) : 32;
+        const uint32_t x = window16(qs, row) ^ window16(rs, col);
+        const int ml = x ? (__clz((int)x) >> 1) : 16;
         const int lim = min(qlen - row, rlen - col);
         if (ml >= lim)
             return row + lim;
         row += ml;
         col += ml;
-        if (ml < 32)
+        if (ml < 16)
             break;
     }
     return row;
@@ -82,12 +90,11 @@ __device__ __forceinline__ int32_t extend_run(const uint64_t *qw, int32_t qlast,
 // of all U are loaded together; a diagonal whose whole window matched goes on
 // in extend_run.
 template <int U>
-__device__ __forceinline__ void extend_u(const uint64_t *qw, int32_t qlast, int32_t qlen,
-                                         const uint64_t *rw, int32_t rlast, int32_t rlen,
-                                         int32_t (&rows)[U], const int32_t (&ks)[U],
+__device__ __forceinline__ void extend_u(const SeqHalves &qs, int32_t qlen, const SeqHalves &rs,
+                                         int32_t rlen, int32_t (&rows)[U], const int32_t (&ks)[U],
                                          const bool (&live)[U])
 {
-    uint64_t x[U];
+    uint32_t x[U];
     int32_t lim[U];
     bool go[U];
 #pragma unroll
@@ -97,21 +104,41 @@ __device__ __forceinline__ void extend_u(const uint64_t *qw, int32_t qlast, int3
         lim[u] = go[u] ? min(qlen - rows[u], rlen - col) : 0;
         x[u] = 0;
         if (go[u])
-            x[u] = window64(qw, qlast, rows[u]) ^ window64(rw, rlast, col);
+            x[u] = window16(qs, rows[u]) ^ window16(rs, col);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         if (!go[u])
             continue;
-        const int ml = x[u] ? (__clzll((long long)x[u]) >> 1) : 32;
+        const int ml = x[u] ? (__clz((int)x[u]) >> 1) : 16;
         if (ml >= lim[u]) {
             rows[u] += lim[u];
         } else {
             rows[u] += ml;
-            if (ml == 32)
-                rows[u] = extend_run(qw, qlast, qlen, rw, rlast, rlen, rows[u], ks[u]);
+            if (ml == 16)
+                rows[u] = extend_run(qs, qlen, rs, rlen, rows[u], ks[u]);
         }
     }
+}
+
+// Copy of one sequence's packed words into shared memory as halves, high
+// half first, plus a zero pad word; or, when it does not fit, a view of the
+// words in global memory.
+template <int TW>
+__device__ __forceinline__ SeqHalves stage_sequence(const SeqView &v, int64_t off, int32_t nw,
+                                                    uint32_t *smem, int seqw, int tt)
+{
+    if (nw < seqw) {
+        uint2 *d = reinterpret_cast<uint2 *>(smem);
+        for (int i = tt; i <= nw; i += TW) {
+            const uint64_t x = i < nw ? __ldg(v.packed + off + i) : 0;
+            d[i] = make_uint2((uint32_t)(x >> 32), (uint32_t)x);
+        }
+        return SeqHalves{smem, 2 * nw, 0u};
+    }
+    const int64_t last = 2 * (v.n_words - off) - 1;
+    return SeqHalves{reinterpret_cast<const uint32_t *>(v.packed + off),
+                     (int32_t)min(last, (int64_t)0x7fffffff), 1u};
 }
 
 // Pair alignment by a team of TEAM warps (TEAM = 1: one warp; TEAM = 4: the
@@ -133,7 +160,8 @@ __device__ __forceinline__ void extend_u(const uint64_t *qw, int32_t qlast, int3
 //    steps filled, and a step needs one team barrier (which also ORs the
 //    "target reached" flags).
 // Both sequences are copied into shared memory when each fits seqw - 1
-// words; longer ones are read from global memory.
+// words; longer ones are read from global memory.  (seqw counts 64-bit
+// words; the copies are stored as 32-bit halves.)
 constexpr int kWfaSeqWords = 321;  // per sequence per warp: 10,240 bases + a zero pad
 constexpr int kWfaWiden = 30;
 constexpr int kWfaTeamSeqWords = 4 * kWfaSeqWords;  // team mode: 41,056 bases + pad
@@ -166,7 +194,7 @@ template <int U, int TEAM>
 __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &r,
                                                const WfaParams &p, const WfaShape &w,
                                                int64_t pi, int32_t *region, int64_t slot_width,
-                                               uint64_t *sq, uint64_t *sr, int seqw,
+                                               uint32_t *sq, uint32_t *sr, int seqw,
                                                int32_t *__restrict__ out, int *err_flag,
                                                int64_t *work)
 {
@@ -189,27 +217,9 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         result = -2;
     } else {
         const int32_t qnw = (qlen + 31) >> 5, rnw = (rlen + 31) >> 5;
-        const uint64_t *qw, *rw;
-        int32_t qlast, rlast;
         team_sync<TEAM>();  // the previous pair's reads of the shared copies are done
-        if (qnw < seqw) {
-            for (int i = tt; i <= qnw; i += TW)
-                sq[i] = i < qnw ? __ldg(q.packed + qoff + i) : 0;
-            qw = sq;
-            qlast = qnw;
-        } else {
-            qw = q.packed + qoff;
-            qlast = (int32_t)min(q.n_words - 1 - qoff, (int64_t)0x7fffffff);
-        }
-        if (rnw < seqw) {
-            for (int i = tt; i <= rnw; i += TW)
-                sr[i] = i < rnw ? __ldg(r.packed + roff + i) : 0;
-            rw = sr;
-            rlast = rnw;
-        } else {
-            rw = r.packed + roff;
-            rlast = (int32_t)min(r.n_words - 1 - roff, (int64_t)0x7fffffff);
-        }
+        const SeqHalves qs = stage_sequence<TW>(q, qoff, qnw, sq, seqw, tt);
+        const SeqHalves rs = stage_sequence<TW>(r, roff, rnw, sr, seqw, tt);
         const int32_t kofs = rlen + 2;
         const int32_t target = qlen - rlen;
         int32_t *const base = region + kofs;
@@ -228,7 +238,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         team_sync<TEAM>();
         // score 0: M[0,0] = 0 extended along diagonal 0 (:130-140); every
         // thread computes it, thread 0 stores it
-        const int32_t row0 = extend_run(qw, qlast, qlen, rw, rlast, rlen, 0, 0);
+        const int32_t row0 = extend_run(qs, qlen, rs, rlen, 0, 0);
         if (lane == 0) {
             mlo = 0;
             mhi = 0;
@@ -331,7 +341,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                             const int32_t m1 = max(m0, max(iv[u], d0));
                             mv[u] = m1 < 0 ? WFA_NEG : m1;
                         }
-                        extend_u<U>(qw, qlast, qlen, rw, rlast, rlen, mv, ks, live);
+                        extend_u<U>(qs, qlen, rs, rlen, mv, ks, live);
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             if (live[u]) {
@@ -394,7 +404,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
            int32_t *__restrict__ out, int32_t *__restrict__ scratch, int64_t slot_width,
            int *err_flag, int64_t *work)
 {
-    __shared__ uint64_t seqs[4 * 2 * kWfaSeqWords];
+    __shared__ __align__(16) uint32_t seqs[4 * 2 * 2 * kWfaSeqWords];
     __shared__ int64_t team_slot;
     WfaShape w;
     w.g = gcd_i(p.x, gcd_i(p.o, p.e));
@@ -421,7 +431,8 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
                 break;
             const int64_t pi = lq ? (int64_t)lq[si] : si;
             wfa_align_pair<U, 4>(q, r, p, w, pi, region, slot_width, seqs,
-                                 seqs + kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag, work);
+                                 seqs + 2 * kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag,
+                                 work);
         }
         __syncthreads();  // shared copies of the last long pair are no longer read
     }
@@ -429,7 +440,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
     int64_t ns;
     const int32_t *__restrict__ sq = pairs_resolve(shorts, ns);
     int32_t *const region = scratch + ((int64_t)blockIdx.x * 4 + wib) * region_words;
-    uint64_t *const my = seqs + (int64_t)wib * 2 * kWfaSeqWords;
+    uint32_t *const my = seqs + wib * 4 * kWfaSeqWords;
     for (;;) {
         int64_t b0 = 0;
         if (lane == 0)
@@ -438,7 +449,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
         if (si >= ns)
             break;
         const int64_t pi = sq ? (int64_t)sq[si] : si;
-        wfa_align_pair<U, 1>(q, r, p, w, pi, region, slot_width, my, my + kWfaSeqWords,
+        wfa_align_pair<U, 1>(q, r, p, w, pi, region, slot_width, my, my + 2 * kWfaSeqWords,
                              kWfaSeqWords, out, err_flag, work);
     }
 }
