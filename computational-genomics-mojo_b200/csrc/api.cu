@@ -649,132 +649,126 @@ struct HostSide {
     const int64_t *lengths;
 };
 
-// Word range [w0, w1) covering pairs [p0, p1) of an append-layout side.
-static void word_range(const HostSide &h, int64_t p0, int64_t p1, int64_t &w0, int64_t &w1)
-{
-    w0 = h.offsets[p0];
-    w1 = h.offsets[p1 - 1] + words_for(h.lengths[p1 - 1]);
-    if (w1 < w0)
-        w1 = w0;
-}
-
-// One pass over the host arrays of both sides: longest sequence, last word
-// touched, whether each side follows add_sequence's append layout
-// (genomics/core/sequence.mojo:44-66: every sequence starts at or after the
-// end of the previous one, so a run of pairs maps to one contiguous word
-// range) and whether any offset or length is negative.  Large batches are
-// split over a few host threads.
-struct HostScan {
-    int64_t qmaxlen = 0, rmaxlen = 0, qmaxword = 0, rmaxword = 0;
-    bool q_append = true, r_append = true, negative = false;
+// One host pass over a chunk's pairs, per side: the word range the chunk's
+// sequences occupy ([smallest offset, largest end), so any layout works --
+// add_sequence's append layout (genomics/core/sequence.mojo:44-66) makes it
+// the chunk's own contiguous run of words), the longest sequence and whether
+// any offset or length is negative.  Large chunks are split over two threads.
+struct ChunkScan {
+    int64_t qw0, qw1, rw0, rw1, qmaxlen, rmaxlen;
+    bool negative;
 };
 
-static void scan_range(const HostSide &hq, const HostSide &hr, int64_t i0, int64_t i1,
-                       HostScan &o)
+static void scan_side(const HostSide &h, int64_t i0, int64_t i1, int64_t &w0, int64_t &w1,
+                      int64_t &maxlen, int64_t &bits)
 {
-    int64_t qprev = i0 > 0 ? hq.offsets[i0 - 1] + words_for(hq.lengths[i0 - 1]) : 0;
-    int64_t rprev = i0 > 0 ? hr.offsets[i0 - 1] + words_for(hr.lengths[i0 - 1]) : 0;
+    int64_t lo = INT64_MAX, hi = 0, mx = 0, b = 0;
     for (int64_t i = i0; i < i1; ++i) {
-        const int64_t qo = hq.offsets[i], ql = hq.lengths[i];
-        const int64_t ro = hr.offsets[i], rl = hr.lengths[i];
-        o.negative |= (qo | ql | ro | rl) < 0;
-        const int64_t qe = qo + words_for(ql), re = ro + words_for(rl);
-        o.q_append &= qo >= qprev;
-        o.r_append &= ro >= rprev;
-        qprev = qe;
-        rprev = re;
-        o.qmaxlen = std::max(o.qmaxlen, ql);
-        o.rmaxlen = std::max(o.rmaxlen, rl);
-        o.qmaxword = std::max(o.qmaxword, qe);
-        o.rmaxword = std::max(o.rmaxword, re);
+        const int64_t o = h.offsets[i], l = h.lengths[i];
+        b |= o | l;
+        mx = l > mx ? l : mx;
+        lo = o < lo ? o : lo;
+        const int64_t e = o + ((l + 31) >> 5);
+        hi = e > hi ? e : hi;
     }
+    w0 = lo;
+    w1 = hi;
+    maxlen = mx;
+    bits = b;
 }
 
-static HostScan scan_host(const HostSide &hq, const HostSide &hr, int64_t n)
+static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, int64_t p1)
 {
-    const int64_t per = 1 << 18;
-    const int nt = (int)std::min<int64_t>(8, (n + per - 1) / per);
-    std::vector<HostScan> parts(std::max(nt, 1));
-    if (nt <= 1) {
-        scan_range(hq, hr, 0, n, parts[0]);
+    int64_t qlo, qhi, qmx, qb, rlo, rhi, rmx, rb;
+    if (p1 - p0 >= (1 << 16)) {
+        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmx, rb); });
+        scan_side(hq, p0, p1, qlo, qhi, qmx, qb);
+        t.join();
     } else {
-        std::vector<std::thread> th;
-        for (int t = 0; t < nt; ++t)
-            th.emplace_back([&, t] { scan_range(hq, hr, n * t / nt, n * (t + 1) / nt, parts[t]); });
-        for (auto &x : th)
-            x.join();
+        scan_side(hq, p0, p1, qlo, qhi, qmx, qb);
+        scan_side(hr, p0, p1, rlo, rhi, rmx, rb);
     }
-    HostScan o;
-    for (const HostScan &p : parts) {
-        o.qmaxlen = std::max(o.qmaxlen, p.qmaxlen);
-        o.rmaxlen = std::max(o.rmaxlen, p.rmaxlen);
-        o.qmaxword = std::max(o.qmaxword, p.qmaxword);
-        o.rmaxword = std::max(o.rmaxword, p.rmaxword);
-        o.q_append &= p.q_append;
-        o.r_append &= p.r_append;
-        o.negative |= p.negative;
-    }
+    ChunkScan o;
+    o.negative = (qb | rb) < 0;
+    o.qw0 = qlo;
+    o.qw1 = std::max(qhi, qlo);
+    o.rw0 = rlo;
+    o.rw1 = std::max(rhi, rlo);
+    o.qmaxlen = qmx;
+    o.rmaxlen = rmx;
     return o;
 }
 
-// Chunks alternate between the context's two executors, so the kernels of
-// one chunk can fill the GPU while the previous chunk's last blocks drain;
-// copies run on their own stream ahead of both.
+// Chunked host-to-device pipeline.  For each chunk the host scans the
+// chunk's offsets and lengths (while the GPU copies and aligns the previous
+// chunks), copies the word range the chunk touches plus its offsets,
+// lengths and bands on the copy stream, and runs the chunk on one of the
+// context's two executors (alternating, so one chunk's kernels can fill the
+// GPU while the previous chunk's last blocks drain); results come back on
+// the executor's stream.  On any error every stream is drained before
+// returning, so no copy touches the caller's memory after the call.
 template <typename RunChunk>
-static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const HostScan &sc,
-                    const int32_t *bands, int64_t n, size_t out_elem, void *out_host,
-                    int64_t chunk_pairs, RunChunk run_chunk)
+static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const int32_t *bands,
+                    int64_t n, size_t out_elem, void *out_host, int64_t chunk_pairs,
+                    RunChunk run_chunk)
 {
-    if (sc.negative)
-        return set_err(c, GB2_EINVAL, "negative offset or length");
-    const bool append = sc.q_append && sc.r_append;
-    if (!append)
-        chunk_pairs = n;  // one chunk holding every word the pairs touch
     const int64_t nchunks = (n + chunk_pairs - 1) / chunk_pairs;
     int rc = GB2_OK;
     const bool out_pinned = is_pinned(out_host);
     if (!out_pinned && (rc = pin_out(c, (size_t)n * out_elem)))
         return rc;
-    for (int64_t ci = 0; ci < nchunks; ++ci) {
+    auto issue = [&](int64_t ci) -> int {
         PipeSet &ps = c->pipe[ci & 1];
         Exec &x = (ci & 1) ? c->x2 : c->x;
         const int64_t p0 = ci * chunk_pairs, p1 = std::min(n, p0 + chunk_pairs);
         const int64_t m = p1 - p0;
-        int64_t qw0 = 0, qw1 = sc.qmaxword, rw0 = 0, rw1 = sc.rmaxword;
-        if (append) {
-            word_range(hq, p0, p1, qw0, qw1);
-            word_range(hr, p0, p1, rw0, rw1);
-        }
-        const int64_t qn = std::max<int64_t>(qw1 - qw0, 1), rn = std::max<int64_t>(rw1 - rw0, 1);
+        const ChunkScan cs = scan_chunk(hq, hr, p0, p1);
+        if (cs.negative)
+            return set_err(c, GB2_EINVAL, "negative offset or length among pairs %lld-%lld",
+                           (long long)p0, (long long)(p1 - 1));
+        const int64_t qn = std::max<int64_t>(cs.qw1 - cs.qw0, 1);
+        const int64_t rn = std::max<int64_t>(cs.rw1 - cs.rw0, 1);
         // this buffer set's previous chunk must have finished computing
         CU(c, cudaEventSynchronize(ps.done));
-        if ((rc = ensure(c, ps.qw, qn * 8, x.st)) || (rc = ensure(c, ps.rw, rn * 8, x.st)) ||
-            (rc = ensure(c, ps.qo, m * 8, x.st)) || (rc = ensure(c, ps.ql, m * 8, x.st)) ||
-            (rc = ensure(c, ps.ro, m * 8, x.st)) || (rc = ensure(c, ps.rl, m * 8, x.st)) ||
-            (rc = ensure(c, ps.out, m * out_elem, x.st)) ||
-            (bands && (rc = ensure(c, ps.bands, m * 4, x.st))))
-            return rc;
-        if ((rc = h2d(c, ps.qw.p, hq.packed + qw0, (size_t)(qw1 - qw0) * 8, c->st_copy)) ||
-            (rc = h2d(c, ps.rw.p, hr.packed + rw0, (size_t)(rw1 - rw0) * 8, c->st_copy)) ||
-            (rc = h2d(c, ps.qo.p, hq.offsets + p0, (size_t)m * 8, c->st_copy)) ||
-            (rc = h2d(c, ps.ql.p, hq.lengths + p0, (size_t)m * 8, c->st_copy)) ||
-            (rc = h2d(c, ps.ro.p, hr.offsets + p0, (size_t)m * 8, c->st_copy)) ||
-            (rc = h2d(c, ps.rl.p, hr.lengths + p0, (size_t)m * 8, c->st_copy)) ||
-            (bands && (rc = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy))))
-            return rc;
+        int r;
+        if ((r = ensure(c, ps.qw, qn * 8, x.st)) || (r = ensure(c, ps.rw, rn * 8, x.st)) ||
+            (r = ensure(c, ps.qo, m * 8, x.st)) || (r = ensure(c, ps.ql, m * 8, x.st)) ||
+            (r = ensure(c, ps.ro, m * 8, x.st)) || (r = ensure(c, ps.rl, m * 8, x.st)) ||
+            (r = ensure(c, ps.out, m * out_elem, x.st)) ||
+            (bands && (r = ensure(c, ps.bands, m * 4, x.st))))
+            return r;
+        if ((r = h2d(c, ps.qw.p, hq.packed + cs.qw0, (size_t)(cs.qw1 - cs.qw0) * 8, c->st_copy)) ||
+            (r = h2d(c, ps.rw.p, hr.packed + cs.rw0, (size_t)(cs.rw1 - cs.rw0) * 8, c->st_copy)) ||
+            (r = h2d(c, ps.qo.p, hq.offsets + p0, (size_t)m * 8, c->st_copy)) ||
+            (r = h2d(c, ps.ql.p, hq.lengths + p0, (size_t)m * 8, c->st_copy)) ||
+            (r = h2d(c, ps.ro.p, hr.offsets + p0, (size_t)m * 8, c->st_copy)) ||
+            (r = h2d(c, ps.rl.p, hr.lengths + p0, (size_t)m * 8, c->st_copy)) ||
+            (bands && (r = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy))))
+            return r;
         CU(c, cudaEventRecord(ps.copied, c->st_copy));
         CU(c, cudaStreamWaitEvent(x.st, ps.copied, 0));
         const SeqView qv{(const uint64_t *)ps.qw.p, (const int64_t *)ps.qo.p,
-                         (const int64_t *)ps.ql.p, qw0, qn};
+                         (const int64_t *)ps.ql.p, cs.qw0, qn};
         const SeqView rv{(const uint64_t *)ps.rw.p, (const int64_t *)ps.ro.p,
-                         (const int64_t *)ps.rl.p, rw0, rn};
-        if ((rc = run_chunk(x, qv, rv, sc.qmaxlen, sc.rmaxlen,
-                            bands ? (const int32_t *)ps.bands.p : nullptr, m, ps.out.p)))
-            return rc;
+                         (const int64_t *)ps.rl.p, cs.rw0, rn};
+        if ((r = run_chunk(x, qv, rv, cs.qmaxlen, cs.rmaxlen,
+                           bands ? (const int32_t *)ps.bands.p : nullptr,
+                           bands ? bands + p0 : nullptr, m, ps.out.p)))
+            return r;
         void *dst = out_pinned ? (char *)out_host + p0 * out_elem
                                : (char *)c->pin_out + p0 * out_elem;
         CU(c, cudaMemcpyAsync(dst, ps.out.p, (size_t)m * out_elem, cudaMemcpyDeviceToHost, x.st));
         CU(c, cudaEventRecord(ps.done, x.st));
+        return GB2_OK;
+    };
+    for (int64_t ci = 0; ci < nchunks && !rc; ++ci)
+        rc = issue(ci);
+    if (rc) {
+        cudaStreamSynchronize(c->st_copy);
+        cudaStreamSynchronize(c->x.st);
+        cudaStreamSynchronize(c->x2.st);
+        cudaGetLastError();
+        return rc;
     }
     CU(c, cudaStreamSynchronize(c->x2.st));
     if ((rc = sync_and_check(c)))
@@ -1053,16 +1047,21 @@ int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_of
     if (n > 0 && (!q_packed || !q_offsets || !q_lengths || !r_packed || !r_offsets ||
                   !r_lengths || !out))
         return set_err(c, GB2_EINVAL, "NULL array");
+    SwPlanInfo pi0;
+    int rc = sw_validate(c, cfg, nullptr, 0, 0, 0, pi0);  // the config alone
+    if (rc || n <= 0)
+        return n < 0 ? set_err(c, GB2_EINVAL, "n_pairs < 0") : rc;
     const HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
-    const HostScan sc = scan_host(hq, hr, std::max<int64_t>(n, 0));
-    SwPlanInfo pi;
-    int rc = sw_validate(c, cfg, bands, n, sc.qmaxlen, sc.rmaxlen, pi);
-    if (rc || n == 0)
-        return rc;
-    const int64_t chunk = std::max<int64_t>(4096, (n + 7) / 8);
-    return pipeline(c, hq, hr, sc, bands, n, sizeof(gb2_sw_result), out, chunk,
+    const int nch = (flags >> 16) & 0xff;
+    const int64_t chunk = nch ? std::max<int64_t>(1, (n + nch - 1) / nch)
+                              : std::max<int64_t>(4096, (n + 7) / 8);
+    return pipeline(c, hq, hr, bands, n, sizeof(gb2_sw_result), out, chunk,
                     [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm,
-                        const int32_t *db, int64_t m, void *dout) {
+                        const int32_t *db, const int32_t *hb, int64_t m, void *dout) {
+                        SwPlanInfo pi;
+                        int r = sw_validate(c, cfg, hb, m, qm, rm, pi);
+                        if (r)
+                            return r;
                         return sw_core(c, x, qv, rv, qm, rm, cfg, db, pi, m,
                                        (gb2_sw_result *)dout, flags);
                     });
@@ -1123,13 +1122,14 @@ int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_o
     if (rc || n == 0)
         return rc;
     const HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
-    const HostScan sc = scan_host(hq, hr, n);
-    const int64_t chunk = std::max<int64_t>(1024, (n + 3) / 4);
+    const int nch = (flags >> 16) & 0xff;
+    const int64_t chunk = nch ? std::max<int64_t>(1, (n + nch - 1) / nch)
+                              : std::max<int64_t>(1024, (n + 3) / 4);
     if ((rc = wfa_begin(c, c->x)) || (rc = wfa_begin(c, c->x2)))
         return rc;
-    rc = pipeline(c, hq, hr, sc, nullptr, n, 4, out, chunk,
+    rc = pipeline(c, hq, hr, nullptr, n, 4, out, chunk,
                   [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, const int32_t *,
-                      int64_t m, void *dout) {
+                      const int32_t *, int64_t m, void *dout) {
                       return wfa_core(c, x, qv, rv, qm, rm, cfg, m, (int32_t *)dout, flags);
                   });
     if (rc)

@@ -76,6 +76,11 @@ typedef struct gb2_batch gb2_batch;
 #define GB2_FLAG_BATCHED 0x1   /* length-bucketed device work queue, persistent kernel */
 #define GB2_FLAG_INT32 0x2     /* never take the packed int16 Smith-Waterman path */
 #define GB2_FLAG_GENERIC 0x4   /* force the literal per-pair kernel (testing) */
+/* Tuning fields (0 = the library's choice): bits 8-15 select a kernel
+ * variant; bits 16-23 set how many chunks the *_host entry points split a
+ * batch into for their copy/compute pipeline. */
+#define GB2_FLAGS_VARIANT(v) (((v) & 0xff) << 8)
+#define GB2_FLAGS_CHUNKS(n) (((n) & 0xff) << 16)
 
 /* ---- library ----------------------------------------------------------------- */
 

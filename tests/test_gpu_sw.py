@@ -249,3 +249,51 @@ def test_device_packing_matches_add_sequence(device, oracle):
     dr = device.upload_batch(r)
     assert_same(device.sw_banded(dq, dr, CFG0, bands=bands), oracle_sw(oracle, q, r, CFG0, bands=bands),
                 "device-packed queries")
+
+
+def _permuted_layout(b: SequenceBatch, rng):
+    """The same sequences stored in a shuffled order of the word array, with
+    one gap word between them: offsets no longer ascend."""
+    p, m, o, l = b.arrays()
+    perm = list(range(len(l)))
+    rng.shuffle(perm)
+    words, masks, offs = [], [], np.zeros(len(l), np.int64)
+    w = 0
+    for i in perm:
+        nw = (int(l[i]) + 31) // 32
+        offs[i] = w
+        words.append(p[o[i]:o[i] + nw])
+        masks.append(m[o[i]:o[i] + nw])
+        words.append(np.zeros(1, np.uint64))
+        masks.append(np.zeros(1, np.uint64))
+        w += nw + 1
+    return SequenceBatch.from_arrays(np.concatenate(words), np.concatenate(masks), offs,
+                                     l.copy())
+
+
+def test_host_pipeline_layouts_and_chunks(device, oracle):
+    """The host entry point over any layout (shuffled offsets, gaps, one
+    sequence shared by several pairs), split into 1..many chunks, equals the
+    resident path and the oracle; a bad length in a late chunk is an error
+    that leaves the context usable."""
+    rng = random.Random(77)
+    q, r = _random_pairs(rng, 3000, 300)
+    cfg = AlignConfig(2, -4, -4, -2, 24)
+    ref = oracle_sw(oracle, q, r, cfg)
+    qs, rs = _permuted_layout(q, rng), _permuted_layout(r, rng)
+    for ch in (0, 1, 3, 7, 64):
+        assert_same(device.sw_banded(qs, rs, cfg, flags=ch << 16), ref, f"chunks {ch}")
+    # pairs 10..19 all use the reference sequence of pair 10
+    p, m, o, l = rs.arrays()
+    o2, l2 = o.copy(), l.copy()
+    o2[10:20], l2[10:20] = o[10], l[10]
+    shared = SequenceBatch.from_arrays(p, m, o2, l2)
+    got = device.sw_banded(qs, shared, cfg, flags=5 << 16)
+    ref2 = oracle_sw(oracle, q, SequenceBatch.from_arrays(p, m, o2, l2), cfg)
+    assert_same(got, ref2, "shared sequence")
+    # a negative length among the last pairs: error, then a clean call
+    bad_l = l.copy()
+    bad_l[-3] = -1
+    with pytest.raises(GenomicsError):
+        device.sw_banded(qs, SequenceBatch.from_arrays(p, m, o, bad_l), cfg, flags=4 << 16)
+    assert_same(device.sw_banded(qs, rs, cfg, flags=4 << 16), ref, "after the error")
