@@ -345,15 +345,26 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
     const bool pack = pi.pack_ok && !force_literal && !(flags & GB2_FLAG_INT32);
     const bool pack_lengths = (int64_t)match_pos * std::min(qmax, rmax) <= kPackHmax;
     // One band for every pair, pairs in input order: no planning kernels.
-    if (pi.uniform_band && !batched) {
+    // The batched path takes it too when the lengths are narrow (nothing to
+    // sort), with a dynamic pair counter.
+    if (pi.uniform_band && (!batched || pi.narrow_lengths)) {
         int cls = (pi.fast_ok && lengths_ok && !force_literal) ? classify_band(cfg->band_width) : 0;
         if ((cls == 16 || cls == 32) && pack && pack_lengths)
             cls |= kPack16;
         PairList pl{nullptr, n, nullptr, nullptr};
+        int grid = 0;  // one pair per thread, pairs in input order
+        if (batched && cls > 0) {  // persistent blocks taking pairs from a counter
+            int rc;
+            if ((rc = ensure(c, x.counters, kCounterBytes, x.st)))
+                return rc;
+            CU(c, cudaMemsetAsync(x.counters.p, 0, 64, x.st));
+            pl.counter = (int *)x.counters.p;
+            grid = c->sm_count * sw_blocks_per_sm(cls, variant);
+        }
         cudaEvent_t e0 = prof_begin(c, x.st);
         if (cls > 0) {
             CU(c, launch_sw(cls, variant, qv, rv, p, cfg->band_width, nullptr, pl, d_out, nullptr,
-                            0, 0, x.st));
+                            0, grid, x.st));
         } else {
             const int rc = ensure_lit();
             if (rc)
@@ -656,37 +667,39 @@ struct HostSide {
 // any offset or length is negative.  Large chunks are split over two threads.
 struct ChunkScan {
     int64_t qw0, qw1, rw0, rw1, qmaxlen, rmaxlen;
-    bool negative;
+    bool negative, narrow;  // narrow: every length within narrow_range
 };
 
 static void scan_side(const HostSide &h, int64_t i0, int64_t i1, int64_t &w0, int64_t &w1,
-                      int64_t &maxlen, int64_t &bits)
+                      int64_t &minlen, int64_t &maxlen, int64_t &bits)
 {
-    int64_t lo = INT64_MAX, hi = 0, mx = 0, b = 0;
+    int64_t lo = INT64_MAX, hi = 0, mn = INT64_MAX, mx = 0, b = 0;
     for (int64_t i = i0; i < i1; ++i) {
         const int64_t o = h.offsets[i], l = h.lengths[i];
         b |= o | l;
         mx = l > mx ? l : mx;
+        mn = l < mn ? l : mn;
         lo = o < lo ? o : lo;
         const int64_t e = o + ((l + 31) >> 5);
         hi = e > hi ? e : hi;
     }
     w0 = lo;
     w1 = hi;
+    minlen = mn;
     maxlen = mx;
     bits = b;
 }
 
 static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, int64_t p1)
 {
-    int64_t qlo, qhi, qmx, qb, rlo, rhi, rmx, rb;
+    int64_t qlo, qhi, qmn, qmx, qb, rlo, rhi, rmn, rmx, rb;
     if (p1 - p0 >= (1 << 16)) {
-        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmx, rb); });
-        scan_side(hq, p0, p1, qlo, qhi, qmx, qb);
+        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb); });
+        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb);
         t.join();
     } else {
-        scan_side(hq, p0, p1, qlo, qhi, qmx, qb);
-        scan_side(hr, p0, p1, rlo, rhi, rmx, rb);
+        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb);
+        scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb);
     }
     ChunkScan o;
     o.negative = (qb | rb) < 0;
@@ -696,6 +709,7 @@ static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, 
     o.rw1 = std::max(rhi, rlo);
     o.qmaxlen = qmx;
     o.rmaxlen = rmx;
+    o.narrow = narrow_range(qmn, qmx) && narrow_range(rmn, rmx);
     return o;
 }
 
@@ -751,7 +765,7 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
                          (const int64_t *)ps.ql.p, cs.qw0, qn};
         const SeqView rv{(const uint64_t *)ps.rw.p, (const int64_t *)ps.ro.p,
                          (const int64_t *)ps.rl.p, cs.rw0, rn};
-        if ((r = run_chunk(x, qv, rv, cs.qmaxlen, cs.rmaxlen,
+        if ((r = run_chunk(x, qv, rv, cs.qmaxlen, cs.rmaxlen, cs.narrow,
                            bands ? (const int32_t *)ps.bands.p : nullptr,
                            bands ? bands + p0 : nullptr, m, ps.out.p)))
             return r;
@@ -920,18 +934,20 @@ int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const 
     if (count < 0 || n_words < 0 || (count > 0 && (!offsets || !lengths)) ||
         (n_words > 0 && !packed))
         return set_err(c, GB2_EINVAL, "batch arrays missing or sizes negative");
-    int64_t maxlen = 0;
+    int64_t maxlen = 0, minlen = count > 0 ? INT64_MAX : 0;
     for (int64_t i = 0; i < count; ++i) {
         if (lengths[i] < 0 || offsets[i] < 0 || offsets[i] + words_for(lengths[i]) > n_words)
             return set_err(c, GB2_EINVAL, "sequence %lld lies outside the packed words",
                            (long long)i);
         maxlen = std::max(maxlen, lengths[i]);
+        minlen = std::min(minlen, lengths[i]);
     }
     gb2_batch *b = new gb2_batch();
     b->owner = c;
     b->count = count;
     b->n_words = n_words;
     b->max_len = maxlen;
+    b->min_len = minlen;
     const size_t wb = (size_t)std::max<int64_t>(n_words, 1) * 8;
     const size_t sb = (size_t)std::max<int64_t>(count, 1) * 8;
     cudaError_t e = cudaMalloc(&b->d_packed, wb);
@@ -1016,6 +1032,8 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
         return set_err(c, GB2_EINVAL, "out is NULL");
     SwPlanInfo pi;
     int rc = sw_validate(c, cfg, bands, n, q->max_len, r->max_len, pi);
+    pi.narrow_lengths =
+        narrow_range(q->min_len, q->max_len) && narrow_range(r->min_len, r->max_len);
     if (rc)
         return rc;
     if (n == 0)
@@ -1056,12 +1074,13 @@ int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_of
     const int64_t chunk = nch ? std::max<int64_t>(1, (n + nch - 1) / nch)
                               : std::max<int64_t>(4096, (n + 7) / 8);
     return pipeline(c, hq, hr, bands, n, sizeof(gb2_sw_result), out, chunk,
-                    [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm,
+                    [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, bool narrow,
                         const int32_t *db, const int32_t *hb, int64_t m, void *dout) {
                         SwPlanInfo pi;
                         int r = sw_validate(c, cfg, hb, m, qm, rm, pi);
                         if (r)
                             return r;
+                        pi.narrow_lengths = narrow;
                         return sw_core(c, x, qv, rv, qm, rm, cfg, db, pi, m,
                                        (gb2_sw_result *)dout, flags);
                     });
@@ -1128,8 +1147,8 @@ int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_o
     if ((rc = wfa_begin(c, c->x)) || (rc = wfa_begin(c, c->x2)))
         return rc;
     rc = pipeline(c, hq, hr, nullptr, n, 4, out, chunk,
-                  [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, const int32_t *,
-                      const int32_t *, int64_t m, void *dout) {
+                  [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, bool,
+                      const int32_t *, const int32_t *, int64_t m, void *dout) {
                       return wfa_core(c, x, qv, rv, qm, rm, cfg, m, (int32_t *)dout, flags);
                   });
     if (rc)

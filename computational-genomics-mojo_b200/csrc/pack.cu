@@ -77,7 +77,7 @@ int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
         (ascii_bytes > 0 && !ascii))
         return set_err(c, GB2_EINVAL, "ascii batch arrays missing or sizes negative");
     std::vector<int64_t> woff((size_t)std::max<int64_t>(count, 1));
-    int64_t words = 0, maxlen = 0;
+    int64_t words = 0, maxlen = 0, minlen = count > 0 ? INT64_MAX : 0;
     for (int64_t i = 0; i < count; ++i) {
         if (lengths[i] < 0 || starts[i] < 0 || starts[i] + lengths[i] > ascii_bytes)
             return set_err(c, GB2_EINVAL, "sequence %lld lies outside the ascii buffer",
@@ -85,12 +85,14 @@ int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
         woff[(size_t)i] = words;
         words += words_for(lengths[i]);
         maxlen = std::max(maxlen, lengths[i]);
+        minlen = std::min(minlen, lengths[i]);
     }
     gb2_batch *b = new gb2_batch();
     b->owner = c;
     b->count = count;
     b->n_words = words;
     b->max_len = maxlen;
+    b->min_len = minlen;
     uint8_t *d_ascii = nullptr;
     int64_t *d_starts = nullptr;
     const size_t wb = (size_t)std::max<int64_t>(words, 1) * 8;

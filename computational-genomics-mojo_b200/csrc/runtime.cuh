@@ -1,5 +1,6 @@
 // runtime.cuh -- host runtime types shared by api.cu and server.cu (not installed).
 #pragma once
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <mutex>
@@ -45,7 +46,17 @@ struct SwPlanInfo {
     bool pack_ok;       // the packed int16x2 kernel applies (scores also small)
     int32_t max_band;
     bool uniform_band;  // no per-pair bands
+    // set by the caller when every pair's lengths lie in a narrow range: a
+    // length-sorted queue would order nothing, so the batched path skips it
+    bool narrow_lengths = false;
 };
+
+// Lengths [lo, hi] count as narrow when hi is within 1/8 (at least 16 bases)
+// of lo.
+inline bool narrow_range(int64_t lo, int64_t hi)
+{
+    return hi - lo <= std::max<int64_t>(16, lo / 8);
+}
 
 }  // namespace gb2
 
@@ -54,7 +65,7 @@ struct gb2_batch {
     uint64_t *d_nmask = nullptr;
     int64_t *d_offsets = nullptr;
     int64_t *d_lengths = nullptr;
-    int64_t count = 0, n_words = 0, max_len = 0;
+    int64_t count = 0, n_words = 0, max_len = 0, min_len = 0;
     gb2_ctx *owner = nullptr;
 };
 

@@ -149,6 +149,8 @@ def test_workload1_resident_subset_and_properties(device, oracle):
     got = device.sw_banded(dq, dr, CFG0, batched=True)
     plain = device.sw_banded(dq, dr, CFG0, batched=False)
     assert (got == plain).all()
+    # end to end from the host arrays (chunked pipeline)
+    assert (device.sw_banded(q, r, CFG0) == got).all()
     # size-independent properties over all 1e6 pairs
     assert (got["score"] >= 0).all() and (got["score"] <= 2 * 150).all()
     assert (got["query_end"] < 150).all() and (got["ref_end"] < 200).all()
