@@ -14,9 +14,11 @@ around its origin, 2% substitutions + 0.5% indels, band 32, scores
               from pinned host arrays: host->device copies of the packed words,
               offsets and lengths and the device->host copy of the results are
               inside the timed region.
-  roofline    integer-ALU view of the dominant kernel: cells x 11 int32 ops (the
-              reference recurrence as written) against the lane-op peak measured by
-              the library's own microkernels in the same run; an HBM view beside it.
+  roofline    integer-ALU view of the dominant kernel: cells x ops per cell (11
+              int32 ops for the reference recurrence as written; 5.5 when the
+              packed int16x2 kernel runs, two cells per lane-op) against the
+              lane-op peak measured by the library's own microkernels in the same
+              run; DRAM traffic per launch from an ncu capture; an HBM view beside.
   cpu_baseline  the C oracle (restatement of align_cpu.mojo) on a bounded
               sample of the same workload, all host threads.
 
@@ -50,6 +52,10 @@ WORKLOAD = ("batched banded Smith-Waterman, 1,000,000 pairs, 150 bp query vs 200
 SCORING = (2, -4, -4, -2)
 BAND = 32
 SW_OPS_PER_CELL = 11  # int32 ops per cell of the reference recurrence (align_cpu.mojo:270-296)
+SW_OPS_PER_CELL_PACKED = 5.5  # the same ops on int16x2 lanes: two cells per lane-op
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel on
+# this workload, from the ncu capture summarised in profiles/sw_pack16_kernel_b32_1M_reads.md
+SW_PACKED_TRAFFIC_BYTES = 141.6e6
 
 
 def parse():
@@ -298,7 +304,11 @@ def our_arm(args, dist: Dist):
         else:
             peak_ops = 36600.0  # 148 SMs x 64 lanes x 2 ops (DPX add-max) x 1.965 GHz
         kern_gcups = cells / (kernel_ms * 1e-3) / 1e9
-        achieved_ops = kern_gcups * SW_OPS_PER_CELL
+        # the packed int16x2 kernel takes every pair of this workload (band <= 32,
+        # score bound match*150 <= 511)
+        packed = BAND <= 32 and SCORING[0] * 150 <= 511
+        ops_per_cell = SW_OPS_PER_CELL_PACKED if packed else SW_OPS_PER_CELL
+        achieved_ops = kern_gcups * ops_per_cell
         alg_bytes = h2d - 0 + d2h  # packed words + metadata read, results written
         mp = {}
         mp_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -327,12 +337,14 @@ def our_arm(args, dist: Dist):
             "roofline": {"bound": "int_alu", "achieved": round(achieved_ops, 1),
                          "peak": peak_ops, "unit": "Gop/s",
                          "frac": round(achieved_ops / peak_ops, 4),
-                         "ops_per_cell": SW_OPS_PER_CELL,
+                         "ops_per_cell": ops_per_cell,
+                         "kernel": "sw_pack16_kernel<32>" if packed else "sw_band_kernel<32>",
                          "kernel_ms": round(kernel_ms, 4),
                          "kernel_gcups": round(kern_gcups, 2),
                          "peak_source": "gb2_int_peak microkernels in this run: "
                                         "max(IADD, IMNMX, 2 x DPX viaddmax) lane-ops/s",
-                         "traffic": None,
+                         "traffic": SW_PACKED_TRAFFIC_BYTES if packed else None,
+                         "traffic_unit": "bytes per launch (ncu)",
                          "hbm": {"achieved": round(alg_bytes / (kernel_ms * 1e-3) / 1e9, 2),
                                  "peak": hbm_peak, "unit": "GB/s",
                                  "frac": round(alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, 5),
