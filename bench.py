@@ -73,8 +73,32 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="plain launch instead of the queue")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-band SW, long-pair WFA and per-call measurements")
-    ap.add_argument("--extras-only", action="store_true", help="(tuning) only the extras")
+    ap.add_argument("--wfa-pass", type=int, default=0, metavar="N",
+                    help="(profiling) one batched WFA pass over N pairs of the long-pair "
+                         "WFA workload, then exit")
     return ap.parse_args()
+
+
+def wfa_pass(n):
+    """One batched WFA pass (x4 o6 e2, exact-cover max_error) over the first n pairs of
+    the long-pair workload, timed with CUDA events: the command the WFA profiles use."""
+    from genomics_b200 import GenomicsDevice, WFAConfig, synth
+    dev = GenomicsDevice(0)
+    q, r, _, _ = synth.generate(2, n)
+    me = synth.wfa_max_error_cover(q, r, 4, 6, 2)
+    cfg = WFAConfig(4, 6, 2, me)
+    dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
+    dev.stats_reset()
+    dev.timer_start()
+    out = dev.wfa_affine(dq, dr, cfg, batched=True)
+    ms = dev.timer_stop()
+    assert (out >= 0).all()
+    print(json.dumps({"wfa_pass_pairs": n, "max_error": me, "ms": round(ms, 3),
+                      "pairs_per_s": round(n / (ms * 1e-3), 1),
+                      "wavefront_cells": dev.stats()["work_units"]}), flush=True)
+    dq.close()
+    dr.close()
+    dev.close()
 
 
 # ---------------------------------------------------------------------------------
@@ -541,6 +565,9 @@ def serve_bench(dev, seconds_per_level=4.0, pool_pairs=40_000):
 
 def main():
     args = parse()
+    if args.wfa_pass > 0:
+        wfa_pass(args.wfa_pass)
+        return
     dist = Dist()
     if args.impl == "reference":
         reference_arm(args, dist)
