@@ -526,7 +526,7 @@ int wfa_begin(gb2_ctx *c, Exec &x)
 }
 
 int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
-             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags)
+             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags, int64_t *d_hist)
 {
     if (n <= 0)
         return GB2_OK;
@@ -583,7 +583,8 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     }
     cudaEvent_t e0 = prof_begin(c, x.st);
     CU(c, launch_wfa(variant, qv, rv, p, longs, shorts, d_out, (int32_t *)x.scratch32.p,
-                     slot_width, (int)grid, (int *)x.errflag.p, (int64_t *)x.work.p, x.st));
+                     slot_width, (int)grid, (int *)x.errflag.p, (int64_t *)x.work.p, d_hist,
+                     x.st));
     prof_end(c, e0, x.st);
     c->launches += 1;
     return GB2_OK;
@@ -872,7 +873,11 @@ int gb2_destroy(gb2_ctx *c)
     harvest_profile(c);
     exec_free(c->x);
     exec_free(c->x2);
-    DevBuf *bufs[] = {&c->out_sw, &c->out_wfa, &c->bands, &c->flush};
+    CigarBufs &cb = c->cig;
+    DevBuf *bufs[] = {&c->out_sw,     &c->out_wfa,  &c->bands,     &c->flush,
+                      &cb.cost,       &cb.hist,     &cb.pairs,     &cb.arena_off,
+                      &cb.arena,      &cb.runs,     &cb.run_off,   &cb.run_count,
+                      &cb.out_off,    &cb.out};
     for (DevBuf *b : bufs)
         if (b->p)
             cudaFree(b->p);

@@ -91,9 +91,36 @@ struct WfaParams {
 // slot_width int32.
 // Resident 128-thread blocks per SM of the WFA kernel variant.
 int wfa_blocks_per_sm(int variant);
+// hist (optional): per pair, the bytes of the cell part of its WFA history
+// record (wfa_hist_cell_bytes summed over the visited scores), 0 when the
+// cost is -1.
 cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
                        PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
-                       int grid, int *err_flag, int64_t *work, cudaStream_t st);
+                       int grid, int *err_flag, int64_t *work, int64_t *hist, cudaStream_t st);
+
+// WFA history record of one pair (the CIGAR traceback's input), at a 16-byte
+// aligned offset of an arena: int32 header[3 * S] (per visited score index:
+// first diagonal a, last diagonal b, offset of its cells in 4-byte words from
+// the record start), then per score with a <= b: int32 M-after-extend[w] and
+// uint8 decision[w] padded to 4 bytes (w = b - a + 1).  Decision bits: 0-1
+// source of M before extension (0 none, 1 mismatch, 2 I, 3 D), bit 2 I comes
+// from an I extension (else from an open), bit 3 D comes from a D extension.
+__host__ __device__ inline int64_t wfa_hist_cell_bytes(int64_t w) { return 4 * w + ((w + 3) & ~3); }
+__host__ __device__ inline int64_t wfa_hist_record_bytes(int64_t cell_bytes, int64_t steps)
+{
+    return (12 * steps + cell_bytes + 15) & ~int64_t(15);
+}
+
+// CIGAR pass over pairs pairs[0..n) (cost and history cell bytes from the
+// cost pass, history record at arena + arena_off[pair]); run-length CIGAR ops of pair i go to
+// runs[run_off[i] ..], their count to run_count[i].  A run is len << 2 | op
+// (op 0 '=', 1 'X', 2 'I', 3 'D').
+cudaError_t launch_wfa_cigar(SeqView q, SeqView r, WfaParams p, const int32_t *pairs, int64_t n,
+                             int *counter, const int32_t *cost, const int64_t *hist_cells,
+                             const int64_t *arena_off, uint8_t *arena, int32_t *scratch,
+                             int64_t slot_width, int grid, uint32_t *runs,
+                             const int64_t *run_off, int32_t *run_count, int *err_flag,
+                             cudaStream_t st);
 
 cudaError_t launch_int_peak(int kind, int grid, int block, int iters, uint32_t *sink,
                             cudaStream_t st);

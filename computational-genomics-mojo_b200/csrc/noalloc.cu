@@ -136,7 +136,7 @@ extern "C" int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
     const gb2::PairList none{nullptr, 0, nullptr, counter};
     const gb2::PairList pl{nullptr, n_pairs, nullptr, counter};
     if (gb2::launch_wfa(0, qv, rv, p, none, pl, out_cost, rings, slot_width, (int)blocks,
-                        err_flag, nullptr, st) != cudaSuccess) {
+                        err_flag, nullptr, nullptr, st) != cudaSuccess) {
         cudaGetLastError();
         return GB2_ECUDA;
     }

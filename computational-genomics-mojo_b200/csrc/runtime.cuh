@@ -35,6 +35,12 @@ struct Exec {
     DevBuf keys, queue, counts, seg, counters, scratch64, scratch32, work, errflag;
 };
 
+// Device buffers of the WFA CIGAR entry point (grow-only, per context).
+struct CigarBufs {
+    DevBuf cost, hist, pairs, arena_off, arena, runs, run_off, run_count, out_off, out;
+};
+constexpr int64_t kCigarArenaCap = 16ll << 30;  // WFA history arena, bytes at most
+
 // One set of device buffers of the end-to-end pipeline.
 struct PipeSet {
     DevBuf qw, rw, qo, ql, ro, rl, bands, out;
@@ -86,6 +92,7 @@ struct gb2_ctx {
     void *pin_out = nullptr;
     size_t pin_out_cap = 0;
     gb2::PipeSet pipe[2];
+    gb2::CigarBufs cig;
     // statistics
     std::atomic<bool> profiling{false};
     std::mutex prof_mu;
@@ -130,8 +137,10 @@ int wfa_validate(gb2_ctx *c, const gb2_wfa_cfg *cfg, int64_t n);
 // Clears the WFA error flag and work counter of x (once per call, before the
 // first wfa_core of that call).
 int wfa_begin(gb2_ctx *c, Exec &x);
+// d_hist (optional): per pair, the history cell bytes the CIGAR pass needs.
 int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
-             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags);
+             const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags,
+             int64_t *d_hist = nullptr);
 // Reads back x's WFA error flag and work counter (synchronises x's stream),
 // folds the work into the context's statistics and turns the flag into a status.
 int wfa_end(gb2_ctx *c, Exec &x);

@@ -53,18 +53,30 @@ struct SeqHalves {
     uint32_t swz;
 };
 
-// 16 bases at position pos: one funnel shift of two halves.  Bases past the
+// 16 bases at position pos: one funnel shift of two halves (the shift
+// amount is taken mod 32, so pos << 1 is (pos mod 16) * 2).  Bases past the
 // sequence end never matter: matches are clamped by the remaining lengths.
+// SMEM: the halves are the shared-memory copy, whose zero pad word makes the
+// second half always present -- no clamp, shared addressing.
+template <bool SMEM>
 __device__ __forceinline__ uint32_t window16(const SeqHalves &s, int32_t pos)
 {
     const int32_t j = pos >> 4;
-    const uint32_t hi = s.w[(uint32_t)j ^ s.swz];
-    const uint32_t lo = s.w[(uint32_t)min(j + 1, s.last) ^ s.swz];
-    return __funnelshift_l(lo, hi, (uint32_t)(pos & 15) << 1);
+    uint32_t hi, lo;
+    if (SMEM) {
+        hi = s.w[j];
+        lo = s.w[j + 1];
+    } else {
+        hi = s.w[(uint32_t)j ^ s.swz];
+        lo = s.w[(uint32_t)min(j + 1, s.last) ^ s.swz];
+    }
+    return __funnelshift_l(lo, hi, (uint32_t)pos << 1);
 }
 
 // Extend along diagonal k from row (align_cpu.mojo:208-219): XOR of the two
-// 16-base windows, count leading zeros, clamp by the remaining lengths.
+// 16-base windows, count leading zeros (32 for a full match, so the match
+// length is clz / 2 either way), clamp by the remaining lengths.
+template <bool SMEM>
 __device__ __forceinline__ int32_t extend_run(const SeqHalves &qs, int32_t qlen,
                                               const SeqHalves &rs, int32_t rlen, int32_t row,
                                               int32_t k)
@@ -73,8 +85,8 @@ __device__ __forceinline__ int32_t extend_run(const SeqHalves &qs, int32_t qlen,
         return row;
     int32_t col = row - k;
     while (row < qlen && col < rlen) {
-        const uint32_t x = window16(qs, row) ^ window16(rs, col);
-        const int ml = x ? (__clz((int)x) >> 1) : 16;
+        const uint32_t x = window16<SMEM>(qs, row) ^ window16<SMEM>(rs, col);
+        const int ml = __clz((int)x) >> 1;
         const int lim = min(qlen - row, rlen - col);
         if (ml >= lim)
             return row + lim;
@@ -88,8 +100,9 @@ __device__ __forceinline__ int32_t extend_run(const SeqHalves &qs, int32_t qlen,
 
 // One extend attempt for U diagonals of a thread at once: the first windows
 // of all U are loaded together; a diagonal whose whole window matched goes on
-// in extend_run.
-template <int U>
+// in extend_run.  A row is in range when 0 <= row < qlen and
+// 0 <= row - k < rlen (one unsigned compare each; NEG rows fail).
+template <int U, bool SMEM>
 __device__ __forceinline__ void extend_u(const SeqHalves &qs, int32_t qlen, const SeqHalves &rs,
                                          int32_t rlen, int32_t (&rows)[U], const int32_t (&ks)[U],
                                          const bool (&live)[U])
@@ -99,36 +112,32 @@ __device__ __forceinline__ void extend_u(const SeqHalves &qs, int32_t qlen, cons
     bool go[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int32_t col = rows[u] >= 0 ? rows[u] - ks[u] : -1;
-        go[u] = live[u] && rows[u] >= 0 && col >= 0 && rows[u] < qlen && col < rlen;
-        lim[u] = go[u] ? min(qlen - rows[u], rlen - col) : 0;
+        const int32_t row = rows[u], col = row - ks[u];
+        go[u] = live[u] && (uint32_t)row < (uint32_t)qlen && (uint32_t)col < (uint32_t)rlen;
+        lim[u] = min(qlen - row, rlen - col);
         x[u] = 0;
         if (go[u])
-            x[u] = window16(qs, rows[u]) ^ window16(rs, col);
+            x[u] = window16<SMEM>(qs, row) ^ window16<SMEM>(rs, col);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         if (!go[u])
             continue;
-        const int ml = x[u] ? (__clz((int)x[u]) >> 1) : 16;
-        if (ml >= lim[u]) {
-            rows[u] += lim[u];
-        } else {
-            rows[u] += ml;
-            if (ml == 16)
-                rows[u] = extend_run(qs, qlen, rs, rlen, rows[u], ks[u]);
-        }
+        const int ml = __clz((int)x[u]) >> 1;
+        rows[u] += min(ml, lim[u]);
+        if (ml == 16 && lim[u] > 16)
+            rows[u] = extend_run<SMEM>(qs, qlen, rs, rlen, rows[u], ks[u]);
     }
 }
 
-// Copy of one sequence's packed words into shared memory as halves, high
-// half first, plus a zero pad word; or, when it does not fit, a view of the
-// words in global memory.
-template <int TW>
+// SMEM: both sequences are copied into shared memory as halves, high half
+// first, plus a zero pad word (the caller checked they fit); otherwise both
+// are read from their packed words in global memory.
+template <int TW, bool SMEM>
 __device__ __forceinline__ SeqHalves stage_sequence(const SeqView &v, int64_t off, int32_t nw,
-                                                    uint32_t *smem, int seqw, int tt)
+                                                    uint32_t *smem, int tt)
 {
-    if (nw < seqw) {
+    if (SMEM) {
         uint2 *d = reinterpret_cast<uint2 *>(smem);
         for (int i = tt; i <= nw; i += TW) {
             const uint64_t x = i < nw ? __ldg(v.packed + off + i) : 0;
@@ -159,8 +168,8 @@ __device__ __forceinline__ SeqHalves stage_sequence(const SeqView &v, int64_t of
 //    reads one more on each side, so its reads stay inside what earlier
 //    steps filled, and a step needs one team barrier (which also ORs the
 //    "target reached" flags).
-// Both sequences are copied into shared memory when each fits seqw - 1
-// words; longer ones are read from global memory.  (seqw counts 64-bit
+// Both sequences are copied into shared memory when both fit seqw - 1 words
+// (SMEM); otherwise both are read from global memory.  (seqw counts 64-bit
 // words; the copies are stored as 32-bit halves.)
 constexpr int kWfaSeqWords = 321;  // per sequence per warp: 10,240 bases + a zero pad
 constexpr int kWfaWiden = 30;
@@ -190,13 +199,13 @@ struct WfaShape {
     int g, xs, oes, es, hm, hie, nslot;
 };
 
-template <int U, int TEAM>
+template <int U, int TEAM, bool SMEM>
 __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &r,
                                                const WfaParams &p, const WfaShape &w,
                                                int64_t pi, int32_t *region, int64_t slot_width,
-                                               uint32_t *sq, uint32_t *sr, int seqw,
+                                               uint32_t *sq, uint32_t *sr,
                                                int32_t *__restrict__ out, int *err_flag,
-                                               int64_t *work)
+                                               int64_t *work, int64_t *hist)
 {
     constexpr int TW = TEAM * 32;
     const unsigned FULL = 0xffffffffu;
@@ -209,6 +218,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
     const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
     int32_t result = -1;
     int64_t cells = 0;
+    int64_t hbytes = 8;  // history bytes of the visited cells (score 0: one cell)
     if (qlen == 0 && rlen == 0) {
         result = 0;
     } else if ((int64_t)qlen + rlen + 5 > slot_width) {
@@ -218,8 +228,8 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
     } else {
         const int32_t qnw = (qlen + 31) >> 5, rnw = (rlen + 31) >> 5;
         team_sync<TEAM>();  // the previous pair's reads of the shared copies are done
-        const SeqHalves qs = stage_sequence<TW>(q, qoff, qnw, sq, seqw, tt);
-        const SeqHalves rs = stage_sequence<TW>(r, roff, rnw, sr, seqw, tt);
+        const SeqHalves qs = stage_sequence<TW, SMEM>(q, qoff, qnw, sq, tt);
+        const SeqHalves rs = stage_sequence<TW, SMEM>(r, roff, rnw, sr, tt);
         const int32_t kofs = rlen + 2;
         const int32_t target = qlen - rlen;
         int32_t *const base = region + kofs;
@@ -238,7 +248,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         team_sync<TEAM>();
         // score 0: M[0,0] = 0 extended along diagonal 0 (:130-140); every
         // thread computes it, thread 0 stores it
-        const int32_t row0 = extend_run(qs, qlen, rs, rlen, 0, 0);
+        const int32_t row0 = extend_run<SMEM>(qs, qlen, rs, rlen, 0, 0);
         if (lane == 0) {
             mlo = 0;
             mhi = 0;
@@ -313,6 +323,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                 bool hit = false;
                 if (a <= b) {
                     cells += (int64_t)(b - a + 1);
+                    hbytes += wfa_hist_cell_bytes(b - a + 1);
                     const int32_t *Mx = sx >= 0 ? M(sx) : nullptr;
                     const int32_t *Moe = soe >= 0 ? M(soe) : nullptr;
                     const int32_t *Ie = se >= 0 ? I(se) : nullptr;
@@ -341,7 +352,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                             const int32_t m1 = max(m0, max(iv[u], d0));
                             mv[u] = m1 < 0 ? WFA_NEG : m1;
                         }
-                        extend_u<U>(qs, qlen, rs, rlen, mv, ks, live);
+                        extend_u<U, SMEM>(qs, qlen, rs, rlen, mv, ks, live);
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             if (live[u]) {
@@ -389,7 +400,15 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         out[pi] = result;
         if (work)
             atomicAdd((unsigned long long *)work, (unsigned long long)cells);
+        if (hist)
+            hist[pi] = result >= 0 ? hbytes : 0;
     }
+}
+
+// Both sequences of pair pi fit shared-memory copies of seqw words (with the pad).
+__device__ __forceinline__ bool fits_smem(const SeqView &q, const SeqView &r, int64_t pi, int seqw)
+{
+    return ((q.lengths[pi] + 31) >> 5) < seqw && ((r.lengths[pi] + 31) >> 5) < seqw;
 }
 
 // Persistent kernel over two length-sorted queues: every block first takes
@@ -402,7 +421,7 @@ template <int U>
 __global__ void __launch_bounds__(128)
 wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
            int32_t *__restrict__ out, int32_t *__restrict__ scratch, int64_t slot_width,
-           int *err_flag, int64_t *work)
+           int *err_flag, int64_t *work, int64_t *hist)
 {
     __shared__ __align__(16) uint32_t seqs[4 * 2 * 2 * kWfaSeqWords];
     __shared__ int64_t team_slot;
@@ -430,9 +449,14 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
             if (si >= nl)
                 break;
             const int64_t pi = lq ? (int64_t)lq[si] : si;
-            wfa_align_pair<U, 4>(q, r, p, w, pi, region, slot_width, seqs,
-                                 seqs + 2 * kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag,
-                                 work);
+            if (fits_smem(q, r, pi, kWfaTeamSeqWords))
+                wfa_align_pair<U, 4, true>(q, r, p, w, pi, region, slot_width, seqs,
+                                           seqs + 2 * kWfaTeamSeqWords, out, err_flag, work,
+                                           hist);
+            else
+                wfa_align_pair<U, 4, false>(q, r, p, w, pi, region, slot_width, seqs,
+                                            seqs + 2 * kWfaTeamSeqWords, out, err_flag, work,
+                                            hist);
         }
         __syncthreads();  // shared copies of the last long pair are no longer read
     }
@@ -449,8 +473,12 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
         if (si >= ns)
             break;
         const int64_t pi = sq ? (int64_t)sq[si] : si;
-        wfa_align_pair<U, 1>(q, r, p, w, pi, region, slot_width, my, my + 2 * kWfaSeqWords,
-                             kWfaSeqWords, out, err_flag, work);
+        if (fits_smem(q, r, pi, kWfaSeqWords))
+            wfa_align_pair<U, 1, true>(q, r, p, w, pi, region, slot_width, my,
+                                       my + 2 * kWfaSeqWords, out, err_flag, work, hist);
+        else
+            wfa_align_pair<U, 1, false>(q, r, p, w, pi, region, slot_width, my,
+                                        my + 2 * kWfaSeqWords, out, err_flag, work, hist);
     }
 }
 
@@ -473,18 +501,18 @@ int wfa_blocks_per_sm(int variant)
 
 cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
                        PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
-                       int grid, int *err_flag, int64_t *work, cudaStream_t st)
+                       int grid, int *err_flag, int64_t *work, int64_t *hist, cudaStream_t st)
 {
     // variant bits 4-5: diagonals per thread per round 4 (default), 2 or 1
     if (variant & 0x20)
         wfa_kernel<1><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work);
+                                            err_flag, work, hist);
     else if (variant & 0x10)
         wfa_kernel<2><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work);
+                                            err_flag, work, hist);
     else
         wfa_kernel<4><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work);
+                                            err_flag, work, hist);
     return cudaGetLastError();
 }
 

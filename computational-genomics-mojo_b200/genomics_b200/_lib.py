@@ -89,6 +89,10 @@ SIGNATURES = [
     ("gb2_wfa_affine_host", ctypes.c_int,
      [vp, vp, vp, vp, vp, vp, vp, P(WfaCfg), c_i64, vp, ctypes.c_int]),
     ("gb2_wfa_pair", ctypes.c_int, [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32)]),
+    ("gb2_wfa_cigar", ctypes.c_int,
+     [vp, vp, vp, P(WfaCfg), c_i64, vp, vp, c_i64, vp, ctypes.c_int]),
+    ("gb2_wfa_cigar_pair", ctypes.c_int,
+     [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32), ctypes.c_char_p, c_i64]),
     ("gb2_wfa_affine_noalloc", ctypes.c_int,
      [vp, c_i64, vp, vp, vp, c_i64, vp, vp, c_i64, c_i64, P(WfaCfg), c_i64, vp, vp]),
     ("gb2_server_start", ctypes.c_int, [vp, P(ServerCfg), P(vp)]),

@@ -24,6 +24,14 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
 
+_CIGAR_OPS = "=XID"
+
+
+def cigar_string(runs) -> str:
+    """The reference's CIGAR string from runs (len << 2 | op)."""
+    return "".join(f"{int(v) >> 2}{_CIGAR_OPS[int(v) & 3]}" for v in runs)
+
+
 class DeviceBatch:
     """A SequenceBatch resident in device memory (freed with close())."""
 
@@ -184,6 +192,47 @@ class GenomicsDevice:
                                                    _ptr(rp), _ptr(ro), _ptr(rl),
                                                    ctypes.byref(c), n, _ptr(out), fl))
         return out
+
+    def wfa_cigar(self, q, r, cfg, n_pairs=None, flags=0):
+        """Batched wfa_affine_cigar_cpu: (costs int32[n], CIGAR strings) for pairs
+        (q[i], r[i]); '' where the cost is -1 (align_cpu.mojo:380-623)."""
+        owned = []
+        if not isinstance(q, DeviceBatch):
+            q = self.upload_batch(q, with_nmask=False)
+            owned.append(q)
+        if not isinstance(r, DeviceBatch):
+            r = self.upload_batch(r, with_nmask=False)
+            owned.append(r)
+        try:
+            n = min(q.count, r.count) if n_pairs is None else int(n_pairs)
+            cost = np.zeros(max(n, 1), np.int32)
+            offs = np.zeros(n + 1, np.int64)
+            cap = n + 1
+            for b in (q, r):
+                lens = np.zeros(max(b.count, 1), np.int64)
+                self._check(self.L.gb2_batch_download(self.ctx, b.handle, None, None, None,
+                                                      _ptr(lens)))
+                cap += int(lens[:n].sum())
+            runs = np.zeros(cap, np.uint32)
+            self._check(self.L.gb2_wfa_cigar(self.ctx, q.handle, r.handle,
+                                             ctypes.byref(_wfa_cfg(cfg)), n, _ptr(cost),
+                                             _ptr(runs), cap, _ptr(offs), flags))
+        finally:
+            for b in owned:
+                b.close()
+        return cost[:n], [cigar_string(runs[offs[i]:offs[i + 1]]) for i in range(n)]
+
+    def wfa_cigar_pair(self, qwords, qlen, rwords, rlen, cfg):
+        """Per-pair drop-in for wfa_affine_cigar_cpu: (cost, CIGAR string)."""
+        qw = np.ascontiguousarray(qwords, np.uint64)
+        rw = np.ascontiguousarray(rwords, np.uint64)
+        cap = int(qlen) + int(rlen) + 1
+        buf = ctypes.create_string_buffer(8 * cap + 16)
+        cost = ctypes.c_int32()
+        self._check(self.L.gb2_wfa_cigar_pair(self.ctx, _ptr(qw), int(qlen), _ptr(rw), int(rlen),
+                                              ctypes.byref(_wfa_cfg(cfg)), ctypes.byref(cost),
+                                              buf, len(buf)))
+        return int(cost.value), buf.value.decode()
 
     def wfa_pair(self, qwords, qlen, rwords, rlen, cfg) -> int:
         c = _wfa_cfg(cfg)

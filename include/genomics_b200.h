@@ -178,6 +178,30 @@ int gb2_wfa_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
                  const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
                  int32_t *out_cost);
 
+/* ---- gap-affine WFA with CIGAR traceback -----------------------------------------
+ * wfa_affine_cigar_cpu (genomics/cpu/align_cpu.mojo:380-623) over pairs
+ * (q[i], r[i]) of two resident batches.  cost[i] is the gb2_wfa_affine cost
+ * (-1 past max_error, then no CIGAR).  The CIGAR of pair i is
+ * runs[run_offsets[i] .. run_offsets[i+1]), each run len << 2 | op with op
+ * 0 '=', 1 'X', 2 'I', 3 'D' in the reference's order and run-length
+ * encoding (:603-621); run_offsets has n_pairs + 1 entries.  runs_cap is the
+ * capacity of `runs`: sum(qlen + rlen) over the pairs always suffices; when
+ * the runs do not fit, returns GB2_ERANGE with run_offsets[n_pairs] set to the
+ * number needed.  Device history: 5 B per visited wavefront cell + 12 B per
+ * score, in groups that fit half the free device memory (at most 16 GiB);
+ * GB2_ENOMEM when one pair alone does not fit. */
+int gb2_wfa_cigar(gb2_ctx *ctx, const gb2_batch *q, const gb2_batch *r,
+                  const gb2_wfa_cfg *cfg, int64_t n_pairs, int32_t *cost,
+                  uint32_t *runs, int64_t runs_cap, int64_t *run_offsets, int flags);
+
+/* Per-pair drop-in for wfa_affine_cigar_cpu(query, ref_seq, cfg)
+   (align_cpu.mojo:380-384): cost out, and the CIGAR as the reference's string
+   ("2=1X1=", empty when the cost is -1) into cigar[cap]; GB2_ERANGE when cap
+   is too small. */
+int gb2_wfa_cigar_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
+                       const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
+                       int32_t *cost, char *cigar, int64_t cap);
+
 /* ---- gap-affine WFA with no device allocation ------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code whose device memory belongs to a host runtime's own allocator,
