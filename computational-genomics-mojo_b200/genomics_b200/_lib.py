@@ -89,6 +89,8 @@ SIGNATURES = [
     ("gb2_wfa_affine_host", ctypes.c_int,
      [vp, vp, vp, vp, vp, vp, vp, P(WfaCfg), c_i64, vp, ctypes.c_int]),
     ("gb2_wfa_pair", ctypes.c_int, [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32)]),
+    ("gb2_nw_banded", ctypes.c_int, [vp, vp, vp, P(SwCfg), vp, c_i64, vp, ctypes.c_int]),
+    ("gb2_nw_pair", ctypes.c_int, [vp, vp, c_i64, vp, c_i64, P(SwCfg), P(SwResult)]),
     ("gb2_wfa_cigar", ctypes.c_int,
      [vp, vp, vp, P(WfaCfg), c_i64, vp, vp, c_i64, vp, ctypes.c_int]),
     ("gb2_wfa_cigar_pair", ctypes.c_int,

@@ -78,6 +78,22 @@ def smith_waterman_banded(query: SequenceView, reference: SequenceView,
     return AlignResult(score=s, query_start=0, ref_start=0, query_end=qe, ref_end=re_, cigar=[])
 
 
+def needleman_wunsch_banded(query: SequenceView, reference: SequenceView,
+                            cfg: AlignConfig) -> AlignResult:
+    """Banded global alignment of one pair (align_cpu.mojo:312-377, with the band rows
+    sized as its indexing intends), on the GPU: score, ends at (qlen-1, rlen-1)."""
+    s, qe, re_ = default_device().nw_pair(query.packed, query.length, reference.packed,
+                                          reference.length, cfg)
+    return AlignResult(score=s, query_start=0, ref_start=0, query_end=qe, ref_end=re_, cigar=[])
+
+
+def wfa_affine_cigar_cpu(query: SequenceView, ref_seq: SequenceView, cfg: WFAConfig):
+    """Gap-affine WFA with CIGAR traceback of one pair (align_cpu.mojo:380-623), on the
+    GPU: (score, CIGAR string); (-1, '') past cfg.max_error."""
+    return default_device().wfa_cigar_pair(query.packed, query.length, ref_seq.packed,
+                                           ref_seq.length, cfg)
+
+
 def wfa_affine_cpu(query: SequenceView, ref_seq: SequenceView, cfg: WFAConfig) -> int:
     """Gap-affine WFA cost of one pair, or -1 past cfg.max_error
     (align_cpu.mojo:75-226).  The name is the reference's; it runs on the GPU."""

@@ -169,6 +169,38 @@ class GenomicsDevice:
                                        ctypes.byref(c), ctypes.byref(res)))
         return res.score, res.query_end, res.ref_end
 
+    # -- NW -----------------------------------------------------------------------------
+    def nw_banded(self, q, r, cfg, bands=None, n_pairs=None, flags=0):
+        """Batched needleman_wunsch_banded (align_cpu.mojo:312-377, intended semantics):
+        structured array (score, query_end = qlen-1, ref_end = rlen-1)."""
+        owned = []
+        if not isinstance(q, DeviceBatch):
+            q = self.upload_batch(q, with_nmask=False)
+            owned.append(q)
+        if not isinstance(r, DeviceBatch):
+            r = self.upload_batch(r, with_nmask=False)
+            owned.append(r)
+        try:
+            n = min(q.count, r.count) if n_pairs is None else int(n_pairs)
+            out = np.zeros(max(n, 1), SW_RESULT_DTYPE)
+            b = None if bands is None else np.ascontiguousarray(bands, np.int32)
+            self._check(self.L.gb2_nw_banded(self.ctx, q.handle, r.handle,
+                                             ctypes.byref(_sw_cfg(cfg)),
+                                             _ptr(b) if b is not None else None, n, _ptr(out),
+                                             flags))
+        finally:
+            for bb in owned:
+                bb.close()
+        return out[:n]
+
+    def nw_pair(self, qwords, qlen, rwords, rlen, cfg):
+        res = _lib.SwResult()
+        qw = np.ascontiguousarray(qwords, np.uint64)
+        rw = np.ascontiguousarray(rwords, np.uint64)
+        self._check(self.L.gb2_nw_pair(self.ctx, _ptr(qw), int(qlen), _ptr(rw), int(rlen),
+                                       ctypes.byref(_sw_cfg(cfg)), ctypes.byref(res)))
+        return res.score, res.query_end, res.ref_end
+
     # -- WFA ----------------------------------------------------------------------------
     def wfa_affine(self, q, r, cfg, n_pairs=None, batched=True, flags=0, out=None):
         """Batched wfa_affine_cpu over pairs (q[i], r[i]); int32 costs (-1 past

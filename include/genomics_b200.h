@@ -178,6 +178,23 @@ int gb2_wfa_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
                  const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
                  int32_t *out_cost);
 
+/* ---- banded Needleman-Wunsch ------------------------------------------------------
+ * needleman_wunsch_banded (genomics/cpu/align_cpu.mojo:312-377) over pairs
+ * (q[i], r[i]) of two resident batches, with the intended semantics of the
+ * reference (its band rows are created with capacity only and indexed,
+ * :327-341; here they have 2*band+1 elements): out[i] = {score, qlen-1,
+ * rlen-1}, score -1000000 when the final cell lies outside the band.  bands:
+ * optional per-pair band widths (NULL: cfg->band_width).  GB2_ERANGE when a
+ * value could leave int32.  GB2_FLAG_GENERIC forces the int64 literal kernel. */
+int gb2_nw_banded(gb2_ctx *ctx, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
+                  const int32_t *bands, int64_t n_pairs, gb2_sw_result *out, int flags);
+
+/* Per-pair drop-in for needleman_wunsch_banded(query, reference, cfg)
+   (align_cpu.mojo:312-316). */
+int gb2_nw_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
+                const uint64_t *r_words, int64_t rlen, const gb2_sw_cfg *cfg,
+                gb2_sw_result *out);
+
 /* ---- gap-affine WFA with CIGAR traceback -----------------------------------------
  * wfa_affine_cigar_cpu (genomics/cpu/align_cpu.mojo:380-623) over pairs
  * (q[i], r[i]) of two resident batches.  cost[i] is the gb2_wfa_affine cost
