@@ -485,6 +485,60 @@ def extras(args, dev):
         "cpu_sample": f"first {ns} pairs, statement-for-statement port (per-score reset of "
                       f"2*max_error+1 diagonals, as the reference)",
     }
+    # WFA with CIGAR traceback: the first 20,000 pairs of the same workload
+    nc = 20_000
+    qc, rc_, _, _ = synth.generate(2, nc)
+    mec = synth.wfa_max_error_cover(qc, rc_, 4, 6, 2)
+    ccfg = WFAConfig(4, 6, 2, mec)
+    dqc, drc = dev.upload_batch(qc, with_nmask=False), dev.upload_batch(rc_, with_nmask=False)
+    tcig = _time_steps(dev, lambda: dev.wfa_cigar(dqc, drc, ccfg, raw=True), 2, 1)
+    _, runs, _ = dev.wfa_cigar(dqc, drc, ccfg, raw=True)
+    # CPU: the oracle's restatement of wfa_affine_cigar_cpu keeps four int64 arrays of
+    # (max_error+1) x (2 max_error+1); it runs with max_error = each pair's own cost (the
+    # smallest budget that finds it) on the first pairs whose cost is at most 1,500
+    qp, _, qo, ql = qc.arrays()
+    rp, _, ro, rl = rc_.arrays()
+    costs = dev.wfa_affine(dqc, drc, ccfg)
+    sample = [i for i in range(nc) if costs[i] <= 1500][:20]
+    strs = lambda p_, o_, l_: "".join("ACGT"[(int(p_[o_ + k // 32]) >> (62 - 2 * (k % 32))) & 3]
+                                      for k in range(int(l_)))
+    pairs = [(strs(qp, qo[i], ql[i]), strs(rp, ro[i], rl[i]), int(costs[i])) for i in sample]
+    t0 = time.perf_counter()
+    for a, b, c in pairs:
+        O.wfa_cigar(a, b, 4, 6, 2, c)
+    tcc = time.perf_counter() - t0
+    out["wfa_cigar_20k"] = {
+        "workload": "first 20,000 pairs of the long-pair WFA workload, x4 o6 e2, exact-cover "
+                    "max_error; cost + CIGAR runs back on the host",
+        "max_error": mec, "cigar_runs": int(runs.size),
+        "gpu_pairs_per_s": round(nc / (tcig * 1e-3), 1), "gpu_ms": round(tcig, 3),
+        "cpu_pairs_per_s": round(len(pairs) / tcc, 2), "cpu_cores": 1,
+        "cpu_sample": f"{len(pairs)} pairs with cost <= 1500, oracle restatement of "
+                      f"wfa_affine_cigar_cpu with max_error = each pair's cost",
+    }
+    dqc.close()
+    drc.close()
+    # banded Needleman-Wunsch: the 1,000,000 read pairs, band 32 (register kernel)
+    qn, rn, _, _ = synth.generate(1, 1_000_000)
+    ncfg = AlignConfig(2, -4, -4, -2, 32)
+    ncells = synth.sw_cells(qn, 32)
+    dqn, drn = dev.upload_batch(qn, with_nmask=False), dev.upload_batch(rn, with_nmask=False)
+    tnw = _time_steps(dev, lambda: dev.nw_banded(dqn, drn, ncfg), 3, 2)
+    qp, _, qo, ql = qn.arrays()
+    rp, _, ro, rl = rn.arrays()
+    ns = 100_000
+    t0 = time.perf_counter()
+    O.nw_batch(qp, qo[:ns], ql[:ns], rp, ro[:ns], rl[:ns], 2, -4, -4, -2, 32, threads=threads)
+    tcn = time.perf_counter() - t0
+    out["nw_1M_reads_band32"] = {
+        "workload": "the 1,000,000 read pairs of the default SW workload, banded NW, band 32, "
+                    "+2/-4/-4/-2",
+        "cells": ncells, "gpu_gcups": round(ncells / tnw / 1e6, 2), "gpu_ms": round(tnw, 3),
+        "cpu_gcups": round(int((ql[:ns] * 65).sum()) / tcn / 1e9, 3), "cpu_cores": threads,
+        "cpu_sample": f"first {ns} pairs",
+    }
+    dqn.close()
+    drn.close()
     dq.close()
     dr.close()
     out["serving"] = serve_bench(dev)

@@ -225,9 +225,10 @@ class GenomicsDevice:
                                                    ctypes.byref(c), n, _ptr(out), fl))
         return out
 
-    def wfa_cigar(self, q, r, cfg, n_pairs=None, flags=0):
+    def wfa_cigar(self, q, r, cfg, n_pairs=None, flags=0, raw=False):
         """Batched wfa_affine_cigar_cpu: (costs int32[n], CIGAR strings) for pairs
-        (q[i], r[i]); '' where the cost is -1 (align_cpu.mojo:380-623)."""
+        (q[i], r[i]); '' where the cost is -1 (align_cpu.mojo:380-623).  raw=True
+        returns (costs, runs, run_offsets) instead of strings (run = len << 2 | op)."""
         owned = []
         if not isinstance(q, DeviceBatch):
             q = self.upload_batch(q, with_nmask=False)
@@ -252,6 +253,8 @@ class GenomicsDevice:
         finally:
             for b in owned:
                 b.close()
+        if raw:
+            return cost[:n], runs[:offs[n]], offs
         return cost[:n], [cigar_string(runs[offs[i]:offs[i + 1]]) for i in range(n)]
 
     def wfa_cigar_pair(self, qwords, qlen, rwords, rlen, cfg):
