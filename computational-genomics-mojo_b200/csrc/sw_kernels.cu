@@ -371,29 +371,56 @@ sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *_
             uint32_t saved_lowkey = 0;
             int32_t best = 0, bq = 0, bc = 0;
             const int steps = qlen > 0 ? qlen + 1 : 0;
+            // The reference window of row t, r[t-B .. t-B+32*NWIN), as 2-bit codes in
+            // NWIN words: built once here, then slid by one base per row; the base
+            // entering at the bottom comes from `rnext`, the reference word holding
+            // position t-B+32*NWIN, reloaded every 32 rows.  Bases before the
+            // reference start are masked below, bases past its end are never read
+            // by an in-matrix cell; loads are clamped to the packed array.
+            uint64_t win[NWIN];
+            {
+                const int64_t w = roff + ((int64_t)(-B) >> 5);
+                const int sh = (int)((-B) & 31) * 2;
+                uint64_t words[NWIN + 1];
+#pragma unroll
+                for (int i = 0; i <= NWIN; ++i) {
+                    int64_t wi = w + i;
+                    wi = wi < 0 ? 0 : (wi >= r.n_words ? r.n_words - 1 : wi);
+                    words[i] = __ldg(r.packed + wi);
+                }
+#pragma unroll
+                for (int i = 0; i < NWIN; ++i)
+                    win[i] = sh ? ((words[i] << sh) | (words[i + 1] >> (64 - sh))) : words[i];
+            }
+            const int64_t rbase = roff + ((int64_t)(32 * NWIN - B) >> 5);  // word of pos 32*NWIN-B
+            int rsub = (32 * NWIN - B) & 31;  // position of the entering base within rnext
+            int64_t rwi = rbase < r.n_words ? rbase : r.n_words - 1;
+            uint64_t rnext = __ldg(r.packed + rwi);
+            uint64_t qword = 0;
             for (int t = 0; t < steps; ++t) {
                 // equality bits of row t against its window r[t-B .. t+B]
                 uint64_t eqc[NWIN + 1];
                 eqc[NWIN] = 0;
                 if (t < qlen) {
-                    const uint64_t qw = __ldg(q.packed + qoff + (t >> 5));
-                    const uint64_t qrep = ((qw >> (62 - 2 * (t & 31))) & 3u) * 0x5555555555555555ull;
+                    if ((t & 31) == 0)
+                        qword = __ldg(q.packed + qoff + (t >> 5));
+                    const uint64_t qrep = ((qword >> (62 - 2 * (t & 31))) & 3u) * 0x5555555555555555ull;
                     const int64_t ri0 = (int64_t)t - B;
-                    const int64_t w = roff + (ri0 >> 5);
-                    const int sh = (int)(ri0 & 31) * 2;
-                    uint64_t words[NWIN + 1];
-#pragma unroll
-                    for (int i = 0; i <= NWIN; ++i) {
-                        int64_t wi = w + i;
-                        wi = wi < 0 ? 0 : (wi >= r.n_words ? r.n_words - 1 : wi);
-                        words[i] = __ldg(r.packed + wi);
-                    }
 #pragma unroll
                     for (int i = 0; i < NWIN; ++i) {
-                        const uint64_t win =
-                            sh ? ((words[i] << sh) | (words[i + 1] >> (64 - sh))) : words[i];
-                        const uint64_t x = win ^ qrep;
+                        const uint64_t x = win[i] ^ qrep;
                         eqc[i] = ~(x | (x >> 1)) & 0x5555555555555555ull;
+                    }
+                    // slide the window one base for row t+1
+                    const uint64_t enter = (rnext >> (62 - 2 * rsub)) & 3u;
+#pragma unroll
+                    for (int i = 0; i + 1 < NWIN; ++i)
+                        win[i] = (win[i] << 2) | (win[i + 1] >> 62);
+                    win[NWIN - 1] = (win[NWIN - 1] << 2) | enter;
+                    if (++rsub == 32) {
+                        rsub = 0;
+                        ++rwi;
+                        rnext = __ldg(r.packed + (rwi < r.n_words ? rwi : r.n_words - 1));
                     }
                     if (ri0 < 0) {  // columns before the reference start never match
                         const int64_t nneg = -ri0;
