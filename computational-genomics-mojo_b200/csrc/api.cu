@@ -664,17 +664,25 @@ struct HostSide {
 // One host pass over a chunk's pairs, per side: the word range the chunk's
 // sequences occupy ([smallest offset, largest end), so any layout works --
 // add_sequence's append layout (genomics/core/sequence.mojo:44-66) makes it
-// the chunk's own contiguous run of words), the longest sequence and whether
-// any offset or length is negative.  Large chunks are split over two threads.
+// the chunk's own contiguous run of words), the longest and shortest
+// sequence, whether any offset or length is negative, and whether every
+// sequence starts at the word where the previous one ends (then the offsets
+// follow from the lengths and are not copied: the lengths are written here
+// as int32 into pinned staging, and the device rebuilds both int64 arrays).
+// Large chunks are split over two threads.
 struct ChunkScan {
     int64_t qw0, qw1, rw0, rw1, qmaxlen, rmaxlen;
     bool negative, narrow;  // narrow: every length within narrow_range
+    bool dense;             // both sides contiguous, lengths staged as int32
 };
 
 static void scan_side(const HostSide &h, int64_t i0, int64_t i1, int64_t &w0, int64_t &w1,
-                      int64_t &minlen, int64_t &maxlen, int64_t &bits)
+                      int64_t &minlen, int64_t &maxlen, int64_t &bits, bool &contig,
+                      int32_t *len32)
 {
     int64_t lo = INT64_MAX, hi = 0, mn = INT64_MAX, mx = 0, b = 0;
+    int64_t expect = i1 > i0 ? h.offsets[i0] : 0;
+    bool ct = true;
     for (int64_t i = i0; i < i1; ++i) {
         const int64_t o = h.offsets[i], l = h.lengths[i];
         b |= o | l;
@@ -683,24 +691,30 @@ static void scan_side(const HostSide &h, int64_t i0, int64_t i1, int64_t &w0, in
         lo = o < lo ? o : lo;
         const int64_t e = o + ((l + 31) >> 5);
         hi = e > hi ? e : hi;
+        ct &= o == expect;
+        expect = e;
+        len32[i - i0] = (int32_t)l;
     }
     w0 = lo;
     w1 = hi;
     minlen = mn;
     maxlen = mx;
     bits = b;
+    contig = ct;
 }
 
-static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, int64_t p1)
+static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, int64_t p1,
+                            int32_t *q32, int32_t *r32)
 {
     int64_t qlo, qhi, qmn, qmx, qb, rlo, rhi, rmn, rmx, rb;
+    bool qc, rc;
     if (p1 - p0 >= (1 << 16)) {
-        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb); });
-        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb);
+        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb, rc, r32); });
+        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb, qc, q32);
         t.join();
     } else {
-        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb);
-        scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb);
+        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb, qc, q32);
+        scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb, rc, r32);
     }
     ChunkScan o;
     o.negative = (qb | rb) < 0;
@@ -711,17 +725,149 @@ static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, 
     o.qmaxlen = qmx;
     o.rmaxlen = rmx;
     o.narrow = narrow_range(qmn, qmx) && narrow_range(rmn, rmx);
+    o.dense = qc && rc && qmx < (1ll << 31) && rmx < (1ll << 31);
     return o;
 }
 
+// Rebuilds a contiguous chunk's int64 offsets and lengths from its int32
+// lengths: offsets[i] = base + sum of words(lengths[j]) over j < i.  Two
+// launches over tiles of kExpandTile pairs (256 threads x 8 consecutive pairs,
+// coalesced): k_expand_sums writes each tile's word totals, k_expand_write
+// adds the totals of the tiles before its own to a block-wide scan and writes
+// both arrays.
+constexpr int kExpandTile = 2048;
+
+__device__ __forceinline__ int64_t block_sum_256(int64_t v, int64_t *sh)
+{
+    for (int o = 16; o; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int64_t t = 0;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < 8 ? sh[threadIdx.x] : 0;
+        for (int o = 4; o; o >>= 1)
+            t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(256)
+k_expand_sums(int64_t m, const int32_t *__restrict__ q32, const int32_t *__restrict__ r32,
+              int64_t *__restrict__ sums)
+{
+    __shared__ int64_t sh[8];
+    const int64_t i0 = (int64_t)blockIdx.x * kExpandTile + threadIdx.x * 8;
+    int64_t aq = 0, ar = 0;
+    for (int k = 0; k < 8; ++k) {
+        const int64_t i = i0 + k;
+        if (i < m) {
+            aq += ((int64_t)q32[i] + 31) >> 5;
+            ar += ((int64_t)r32[i] + 31) >> 5;
+        }
+    }
+    const int64_t tq = block_sum_256(aq, sh);
+    const int64_t tr = block_sum_256(ar, sh);
+    if (threadIdx.x == 0) {
+        sums[2 * blockIdx.x] = tq;
+        sums[2 * blockIdx.x + 1] = tr;
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_expand_write(int64_t m, const int32_t *__restrict__ q32, const int32_t *__restrict__ r32,
+               const int64_t *__restrict__ sums, int64_t qbase, int64_t rbase,
+               int64_t *__restrict__ qo, int64_t *__restrict__ ql, int64_t *__restrict__ ro,
+               int64_t *__restrict__ rl)
+{
+    __shared__ int64_t sh[8];
+    __shared__ int64_t wq[8], wr[8];
+    // totals of the tiles before this one
+    int64_t pq = 0, pr = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) {
+        pq += sums[2 * b];
+        pr += sums[2 * b + 1];
+    }
+    pq = block_sum_256(pq, sh);
+    pr = block_sum_256(pr, sh);
+    __shared__ int64_t base_q, base_r;
+    if (threadIdx.x == 0) {
+        base_q = qbase + pq;
+        base_r = rbase + pr;
+    }
+    // this thread's 8 pairs, then an exclusive scan over the block
+    const int64_t i0 = (int64_t)blockIdx.x * kExpandTile + threadIdx.x * 8;
+    int32_t lq[8], lr[8];
+    int64_t aq = 0, ar = 0;
+    for (int k = 0; k < 8; ++k) {
+        const int64_t i = i0 + k;
+        lq[k] = i < m ? q32[i] : 0;
+        lr[k] = i < m ? r32[i] : 0;
+        aq += ((int64_t)lq[k] + 31) >> 5;
+        ar += ((int64_t)lr[k] + 31) >> 5;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t xq = aq, xr = ar;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t vq = __shfl_up_sync(0xffffffffu, xq, o);
+        const int64_t vr = __shfl_up_sync(0xffffffffu, xr, o);
+        if (lane >= o) {
+            xq += vq;
+            xr += vr;
+        }
+    }
+    if (lane == 31) {
+        wq[warp] = xq;
+        wr[warp] = xr;
+    }
+    __syncthreads();
+    int64_t oq = base_q + xq - aq, orr = base_r + xr - ar;
+    for (int w = 0; w < warp; ++w) {
+        oq += wq[w];
+        orr += wr[w];
+    }
+    for (int k = 0; k < 8; ++k) {
+        const int64_t i = i0 + k;
+        if (i < m) {
+            qo[i] = oq;
+            ql[i] = lq[k];
+            ro[i] = orr;
+            rl[i] = lr[k];
+        }
+        oq += ((int64_t)lq[k] + 31) >> 5;
+        orr += ((int64_t)lr[k] + 31) >> 5;
+    }
+}
+
+// Grows a pipe set's pinned int32 staging (its previous copy has completed).
+static int ensure_len32(gb2_ctx *c, PipeSet &ps, size_t bytes)
+{
+    if (bytes <= ps.h_len32_cap)
+        return GB2_OK;
+    if (ps.h_len32)
+        cudaFreeHost(ps.h_len32);
+    ps.h_len32 = nullptr;
+    ps.h_len32_cap = 0;
+    const size_t cap = std::max<size_t>(bytes + bytes / 4, 1 << 16);
+    CU(c, cudaMallocHost(&ps.h_len32, cap));
+    ps.h_len32_cap = cap;
+    return GB2_OK;
+}
+
 // Chunked host-to-device pipeline.  For each chunk the host scans the
-// chunk's offsets and lengths (while the GPU copies and aligns the previous
-// chunks), copies the word range the chunk touches plus its offsets,
-// lengths and bands on the copy stream, and runs the chunk on one of the
-// context's two executors (alternating, so one chunk's kernels can fill the
-// GPU while the previous chunk's last blocks drain); results come back on
-// the executor's stream.  On any error every stream is drained before
-// returning, so no copy touches the caller's memory after the call.
+// chunk's offsets and lengths (while the GPU copies and aligns earlier
+// chunks), copies the word range the chunk touches plus its lengths (int32,
+// offsets rebuilt on the device, when the chunk is contiguous; else int64
+// offsets and lengths) and bands on the copy stream, and runs the chunk on
+// one of the context's two executors (alternating, so one chunk's kernels can
+// fill the GPU while the previous chunk's last blocks drain); results come
+// back on the executor's stream.  kPipeSets chunks are in flight: the copies
+// of a chunk wait on the device for the chunk that last used its buffers,
+// and the host waits only before reusing pinned staging that may still be
+// read.  On any error every stream is drained before returning, so no copy
+// touches the caller's memory after the call.
 template <typename RunChunk>
 static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const int32_t *bands,
                     int64_t n, size_t out_elem, void *out_host, int64_t chunk_pairs,
@@ -733,35 +879,64 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
     if (!out_pinned && (rc = pin_out(c, (size_t)n * out_elem)))
         return rc;
     auto issue = [&](int64_t ci) -> int {
-        PipeSet &ps = c->pipe[ci & 1];
+        PipeSet &ps = c->pipe[ci % kPipeSets];
         Exec &x = (ci & 1) ? c->x2 : c->x;
         const int64_t p0 = ci * chunk_pairs, p1 = std::min(n, p0 + chunk_pairs);
         const int64_t m = p1 - p0;
-        const ChunkScan cs = scan_chunk(hq, hr, p0, p1);
+        int r;
+        // the staging of this set's previous chunk has been copied
+        CU(c, cudaEventSynchronize(ps.copied));
+        if ((r = ensure_len32(c, ps, (size_t)m * 8)))
+            return r;
+        int32_t *q32 = (int32_t *)ps.h_len32, *r32 = q32 + m;
+        const ChunkScan cs = scan_chunk(hq, hr, p0, p1, q32, r32);
         if (cs.negative)
             return set_err(c, GB2_EINVAL, "negative offset or length among pairs %lld-%lld",
                            (long long)p0, (long long)(p1 - 1));
         const int64_t qn = std::max<int64_t>(cs.qw1 - cs.qw0, 1);
         const int64_t rn = std::max<int64_t>(cs.rw1 - cs.rw0, 1);
-        // this buffer set's previous chunk must have finished computing
-        CU(c, cudaEventSynchronize(ps.done));
-        int r;
+        const bool grow = ps.qw.cap < (size_t)qn * 8 || ps.rw.cap < (size_t)rn * 8 ||
+                          ps.qo.cap < (size_t)m * 8 || ps.out.cap < (size_t)m * out_elem ||
+                          ps.len32.cap < (size_t)m * 8 + 16 * (m / kExpandTile + 1) ||
+                          (bands && ps.bands.cap < (size_t)m * 4);
+        if (grow)  // reallocating: the set's previous chunk must be completely done
+            CU(c, cudaEventSynchronize(ps.done));
         if ((r = ensure(c, ps.qw, qn * 8, x.st)) || (r = ensure(c, ps.rw, rn * 8, x.st)) ||
             (r = ensure(c, ps.qo, m * 8, x.st)) || (r = ensure(c, ps.ql, m * 8, x.st)) ||
             (r = ensure(c, ps.ro, m * 8, x.st)) || (r = ensure(c, ps.rl, m * 8, x.st)) ||
             (r = ensure(c, ps.out, m * out_elem, x.st)) ||
+            (r = ensure(c, ps.len32, m * 8 + 16 * (m / kExpandTile + 1), x.st)) ||
             (bands && (r = ensure(c, ps.bands, m * 4, x.st))))
             return r;
+        // the device buffers of this set's previous chunk are free once it is done
+        CU(c, cudaStreamWaitEvent(c->st_copy, ps.done, 0));
         if ((r = h2d(c, ps.qw.p, hq.packed + cs.qw0, (size_t)(cs.qw1 - cs.qw0) * 8, c->st_copy)) ||
-            (r = h2d(c, ps.rw.p, hr.packed + cs.rw0, (size_t)(cs.rw1 - cs.rw0) * 8, c->st_copy)) ||
-            (r = h2d(c, ps.qo.p, hq.offsets + p0, (size_t)m * 8, c->st_copy)) ||
-            (r = h2d(c, ps.ql.p, hq.lengths + p0, (size_t)m * 8, c->st_copy)) ||
-            (r = h2d(c, ps.ro.p, hr.offsets + p0, (size_t)m * 8, c->st_copy)) ||
-            (r = h2d(c, ps.rl.p, hr.lengths + p0, (size_t)m * 8, c->st_copy)) ||
-            (bands && (r = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy))))
+            (r = h2d(c, ps.rw.p, hr.packed + cs.rw0, (size_t)(cs.rw1 - cs.rw0) * 8, c->st_copy)))
+            return r;
+        if (cs.dense) {
+            CU(c, cudaMemcpyAsync(ps.len32.p, q32, (size_t)m * 8, cudaMemcpyHostToDevice,
+                                  c->st_copy));
+        } else if ((r = h2d(c, ps.qo.p, hq.offsets + p0, (size_t)m * 8, c->st_copy)) ||
+                   (r = h2d(c, ps.ql.p, hq.lengths + p0, (size_t)m * 8, c->st_copy)) ||
+                   (r = h2d(c, ps.ro.p, hr.offsets + p0, (size_t)m * 8, c->st_copy)) ||
+                   (r = h2d(c, ps.rl.p, hr.lengths + p0, (size_t)m * 8, c->st_copy))) {
+            return r;
+        }
+        if (bands && (r = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy)))
             return r;
         CU(c, cudaEventRecord(ps.copied, c->st_copy));
         CU(c, cudaStreamWaitEvent(x.st, ps.copied, 0));
+        if (cs.dense) {
+            const int32_t *d32 = (const int32_t *)ps.len32.p;
+            int64_t *sums = (int64_t *)((char *)ps.len32.p + (size_t)m * 8);
+            const int tiles = (int)((m + kExpandTile - 1) / kExpandTile);
+            k_expand_sums<<<tiles, 256, 0, x.st>>>(m, d32, d32 + m, sums);
+            k_expand_write<<<tiles, 256, 0, x.st>>>(m, d32, d32 + m, sums, cs.qw0, cs.rw0,
+                                                    (int64_t *)ps.qo.p, (int64_t *)ps.ql.p,
+                                                    (int64_t *)ps.ro.p, (int64_t *)ps.rl.p);
+            CU(c, cudaGetLastError());
+            c->launches += 2;
+        }
         const SeqView qv{(const uint64_t *)ps.qw.p, (const int64_t *)ps.qo.p,
                          (const int64_t *)ps.ql.p, cs.qw0, qn};
         const SeqView rv{(const uint64_t *)ps.rw.p, (const int64_t *)ps.ro.p,
@@ -844,11 +1019,15 @@ int gb2_create(int device, gb2_ctx **out)
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
     for (int i = 0; ok && i < 2; ++i) {
         ok = cudaMallocHost(&c->pin[i], (size_t)kPinChunk) == cudaSuccess &&
-             cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&c->pipe[i].copied, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming) == cudaSuccess;
+        if (ok)
+            cudaEventRecord(c->pin_ev[i], c->x.st);
+    }
+    for (int i = 0; ok && i < kPipeSets; ++i) {
+        ok = cudaEventCreateWithFlags(&c->pipe[i].copied, cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pipe[i].done, cudaEventDisableTiming) == cudaSuccess;
         if (ok) {
-            cudaEventRecord(c->pin_ev[i], c->x.st);
+            cudaEventRecord(c->pipe[i].copied, c->x.st);
             cudaEventRecord(c->pipe[i].done, c->x.st);
         }
     }
@@ -881,16 +1060,21 @@ int gb2_destroy(gb2_ctx *c)
     for (DevBuf *b : bufs)
         if (b->p)
             cudaFree(b->p);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kPipeSets; ++i) {
         PipeSet &ps = c->pipe[i];
-        DevBuf *pb[] = {&ps.qw, &ps.rw, &ps.qo, &ps.ql, &ps.ro, &ps.rl, &ps.bands, &ps.out};
+        DevBuf *pb[] = {&ps.qw, &ps.rw,    &ps.qo,  &ps.ql,   &ps.ro,
+                        &ps.rl, &ps.bands, &ps.out, &ps.len32};
         for (DevBuf *b : pb)
             if (b->p)
                 cudaFree(b->p);
+        if (ps.h_len32)
+            cudaFreeHost(ps.h_len32);
         if (ps.copied)
             cudaEventDestroy(ps.copied);
         if (ps.done)
             cudaEventDestroy(ps.done);
+    }
+    for (int i = 0; i < 2; ++i) {
         if (c->pin[i])
             cudaFreeHost(c->pin[i]);
         if (c->pin_ev[i])
@@ -1076,8 +1260,9 @@ int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_of
         return n < 0 ? set_err(c, GB2_EINVAL, "n_pairs < 0") : rc;
     const HostSide hq{q_packed, q_offsets, q_lengths}, hr{r_packed, r_offsets, r_lengths};
     const int nch = (flags >> 16) & 0xff;
+    // default: 16 chunks of at least 65,536 pairs (a chunk fills the GPU)
     const int64_t chunk = nch ? std::max<int64_t>(1, (n + nch - 1) / nch)
-                              : std::max<int64_t>(4096, (n + 7) / 8);
+                              : std::max<int64_t>(1 << 16, (n + 15) / 16);
     return pipeline(c, hq, hr, bands, n, sizeof(gb2_sw_result), out, chunk,
                     [&](Exec &x, SeqView qv, SeqView rv, int64_t qm, int64_t rm, bool narrow,
                         const int32_t *db, const int32_t *hb, int64_t m, void *dout) {
