@@ -199,7 +199,19 @@ struct WfaShape {
     int g, xs, oes, es, hm, hie, nslot;
 };
 
-template <int U, int TEAM, bool SMEM>
+// Ring element: int32 (NEG = -2^30) or, when every value a pair can store
+// fits (rows <= qlen + max_error/g <= 32767, checked by the caller), int16
+// (NEG = -16384): half the ring bytes.  Arithmetic is int32 either way and
+// negative results are stored as NEG, so both give the same values.
+template <typename RT> struct RingNeg;
+template <> struct RingNeg<int32_t> {
+    static constexpr int32_t value = WFA_NEG;
+};
+template <> struct RingNeg<int16_t> {
+    static constexpr int32_t value = -16384;
+};
+
+template <int U, int TEAM, bool SMEM, typename RT>
 __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &r,
                                                const WfaParams &p, const WfaShape &w,
                                                int64_t pi, int32_t *region, int64_t slot_width,
@@ -208,6 +220,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                                                int64_t *work, int64_t *hist)
 {
     constexpr int TW = TEAM * 32;
+    constexpr int32_t NEG = RingNeg<RT>::value;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int tt = TEAM == 1 ? lane : (int)threadIdx.x;
@@ -232,7 +245,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         const SeqHalves rs = stage_sequence<TW, SMEM>(r, roff, rnw, sr, tt);
         const int32_t kofs = rlen + 2;
         const int32_t target = qlen - rlen;
-        int32_t *const base = region + kofs;
+        RT *const base = reinterpret_cast<RT *>(region) + kofs;
         auto M = [&](int slot) { return base + (int64_t)slot * slot_width; };
         auto I = [&](int slot) { return base + (int64_t)(hm + slot) * slot_width; };
         auto D = [&](int slot) { return base + (int64_t)(hm + hie + slot) * slot_width; };
@@ -241,9 +254,9 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         int32_t mlo = 1, mhi = 0, ilo = 1, ihi = 0;
         int32_t GL = max(-2, -rlen - 2), GH = min(2, qlen + 2);
         for (int sl = 0; sl < w.nslot; ++sl) {
-            int32_t *row = base + (int64_t)sl * slot_width;
+            RT *row = base + (int64_t)sl * slot_width;
             for (int32_t k = GL + tt; k <= GH; k += TW)
-                row[k] = WFA_NEG;
+                row[k] = NEG;
         }
         team_sync<TEAM>();
         // score 0: M[0,0] = 0 extended along diagonal 0 (:130-140); every
@@ -254,7 +267,7 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
             mhi = 0;
         }
         if (tt == 0)
-            M(0)[0] = row0;
+            M(0)[0] = (RT)row0;
         team_sync<TEAM>();
         if (target == 0 && row0 >= qlen) {
             result = 0;
@@ -301,33 +314,33 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                 const int32_t omhi = __shfl_sync(FULL, mhi, ms);
                 const int32_t oilo = __shfl_sync(FULL, ilo, is);
                 const int32_t oihi = __shfl_sync(FULL, ihi, is);
-                int32_t *const Mw = M(ms), *const Iw = I(is), *const Dw = D(is);
+                RT *const Mw = M(ms), *const Iw = I(is), *const Dw = D(is);
                 // what the reused slots held outside [a, b] becomes NEG (all
                 // of it when this score is empty)
                 const int32_t ca = a > b ? 0x7fffffff : a, cb = a > b ? -0x7fffffff : b;
                 if ((omlo <= omhi && (omlo < ca || omhi > cb)) ||
                     (oilo <= oihi && (oilo < ca || oihi > cb))) {
                     for (int32_t k = omlo + tt; k <= min(omhi, ca - 1); k += TW)
-                        Mw[k] = WFA_NEG;
+                        Mw[k] = NEG;
                     for (int32_t k = max(omlo, cb + 1) + tt; k <= omhi; k += TW)
-                        Mw[k] = WFA_NEG;
+                        Mw[k] = NEG;
                     for (int32_t k = oilo + tt; k <= min(oihi, ca - 1); k += TW) {
-                        Iw[k] = WFA_NEG;
-                        Dw[k] = WFA_NEG;
+                        Iw[k] = NEG;
+                        Dw[k] = NEG;
                     }
                     for (int32_t k = max(oilo, cb + 1) + tt; k <= oihi; k += TW) {
-                        Iw[k] = WFA_NEG;
-                        Dw[k] = WFA_NEG;
+                        Iw[k] = NEG;
+                        Dw[k] = NEG;
                     }
                 }
                 bool hit = false;
                 if (a <= b) {
                     cells += (int64_t)(b - a + 1);
                     hbytes += wfa_hist_cell_bytes(b - a + 1);
-                    const int32_t *Mx = sx >= 0 ? M(sx) : nullptr;
-                    const int32_t *Moe = soe >= 0 ? M(soe) : nullptr;
-                    const int32_t *Ie = se >= 0 ? I(se) : nullptr;
-                    const int32_t *De = se >= 0 ? D(se) : nullptr;
+                    const RT *Mx = sx >= 0 ? M(sx) : nullptr;
+                    const RT *Moe = soe >= 0 ? M(soe) : nullptr;
+                    const RT *Ie = se >= 0 ? I(se) : nullptr;
+                    const RT *De = se >= 0 ? D(se) : nullptr;
                     for (int32_t k0 = a + tt; k0 <= b; k0 += TW * U) {
                         int32_t ks[U], iv[U], dv[U], mv[U];
                         bool live[U];
@@ -336,29 +349,29 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                             ks[u] = k0 + TW * u;
                             live[u] = ks[u] <= b;
                             const int32_t kc = live[u] ? ks[u] : b;  // loads stay in [a-1, b+1]
-                            int32_t i0 = WFA_NEG, d0 = WFA_NEG, m0 = WFA_NEG;
+                            int32_t i0 = NEG, d0 = NEG, m0 = NEG;
                             if (Moe) {
-                                i0 = Moe[kc - 1];
-                                d0 = Moe[kc + 1];
+                                i0 = (int32_t)Moe[kc - 1];
+                                d0 = (int32_t)Moe[kc + 1];
                             }
                             if (Ie) {
-                                i0 = max(i0, Ie[kc - 1]);
-                                d0 = max(d0, De[kc + 1]);
+                                i0 = max(i0, (int32_t)Ie[kc - 1]);
+                                d0 = max(d0, (int32_t)De[kc + 1]);
                             }
                             if (Mx)
-                                m0 = Mx[kc] + 1;
-                            iv[u] = i0 < 0 ? WFA_NEG : i0 + 1;
+                                m0 = (int32_t)Mx[kc] + 1;
+                            iv[u] = i0 < 0 ? NEG : i0 + 1;
                             dv[u] = d0;
                             const int32_t m1 = max(m0, max(iv[u], d0));
-                            mv[u] = m1 < 0 ? WFA_NEG : m1;
+                            mv[u] = m1 < 0 ? NEG : m1;
                         }
                         extend_u<U, SMEM>(qs, qlen, rs, rlen, mv, ks, live);
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             if (live[u]) {
-                                Iw[ks[u]] = iv[u];
-                                Dw[ks[u]] = dv[u];
-                                Mw[ks[u]] = mv[u];
+                                Iw[ks[u]] = (RT)iv[u];
+                                Dw[ks[u]] = (RT)dv[u];
+                                Mw[ks[u]] = (RT)mv[u];
                                 hit |= ks[u] == target && mv[u] >= qlen;
                             }
                         }
@@ -369,11 +382,11 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                         const int32_t nGL = a - 2 < GL ? max(a - 2 - kWfaWiden, -rlen - 2) : GL;
                         const int32_t nGH = b + 2 > GH ? min(b + 2 + kWfaWiden, qlen + 2) : GH;
                         for (int sl = 0; sl < w.nslot; ++sl) {
-                            int32_t *rowp = base + (int64_t)sl * slot_width;
+                            RT *rowp = base + (int64_t)sl * slot_width;
                             for (int32_t k = nGL + tt; k < GL; k += TW)
-                                rowp[k] = WFA_NEG;
+                                rowp[k] = NEG;
                             for (int32_t k = GH + 1 + tt; k <= nGH; k += TW)
-                                rowp[k] = WFA_NEG;
+                                rowp[k] = NEG;
                         }
                         GL = nGL;
                         GH = nGH;
@@ -405,10 +418,31 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
     }
 }
 
-// Both sequences of pair pi fit shared-memory copies of seqw words (with the pad).
-__device__ __forceinline__ bool fits_smem(const SeqView &q, const SeqView &r, int64_t pi, int seqw)
+// Runs pair pi with the shared-memory copies when both sequences fit seqw
+// words (with the pad) and with int16 rings when its rows fit them.
+template <int U, int TEAM>
+__device__ __forceinline__ void wfa_pair_dispatch(const SeqView &q, const SeqView &r,
+                                                  const WfaParams &p, const WfaShape &w,
+                                                  int64_t pi, int32_t *region,
+                                                  int64_t slot_width, uint32_t *sq,
+                                                  uint32_t *sr, int seqw, int32_t *out,
+                                                  int *err_flag, int64_t *work, int64_t *hist)
 {
-    return ((q.lengths[pi] + 31) >> 5) < seqw && ((r.lengths[pi] + 31) >> 5) < seqw;
+    const int64_t ql = q.lengths[pi], rl = r.lengths[pi];
+    const bool smem = ((ql + 31) >> 5) < seqw && ((rl + 31) >> 5) < seqw;
+    const bool r16 = ql + p.max_error / w.g <= 32767;
+    if (smem && r16)
+        wfa_align_pair<U, TEAM, true, int16_t>(q, r, p, w, pi, region, slot_width, sq, sr, out,
+                                               err_flag, work, hist);
+    else if (smem)
+        wfa_align_pair<U, TEAM, true, int32_t>(q, r, p, w, pi, region, slot_width, sq, sr, out,
+                                               err_flag, work, hist);
+    else if (r16)
+        wfa_align_pair<U, TEAM, false, int16_t>(q, r, p, w, pi, region, slot_width, sq, sr,
+                                                out, err_flag, work, hist);
+    else
+        wfa_align_pair<U, TEAM, false, int32_t>(q, r, p, w, pi, region, slot_width, sq, sr,
+                                                out, err_flag, work, hist);
 }
 
 // Persistent kernel over two length-sorted queues: every block first takes
@@ -449,14 +483,9 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
             if (si >= nl)
                 break;
             const int64_t pi = lq ? (int64_t)lq[si] : si;
-            if (fits_smem(q, r, pi, kWfaTeamSeqWords))
-                wfa_align_pair<U, 4, true>(q, r, p, w, pi, region, slot_width, seqs,
-                                           seqs + 2 * kWfaTeamSeqWords, out, err_flag, work,
-                                           hist);
-            else
-                wfa_align_pair<U, 4, false>(q, r, p, w, pi, region, slot_width, seqs,
-                                            seqs + 2 * kWfaTeamSeqWords, out, err_flag, work,
-                                            hist);
+            wfa_pair_dispatch<U, 4>(q, r, p, w, pi, region, slot_width, seqs,
+                                    seqs + 2 * kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag,
+                                    work, hist);
         }
         __syncthreads();  // shared copies of the last long pair are no longer read
     }
@@ -473,12 +502,8 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
         if (si >= ns)
             break;
         const int64_t pi = sq ? (int64_t)sq[si] : si;
-        if (fits_smem(q, r, pi, kWfaSeqWords))
-            wfa_align_pair<U, 1, true>(q, r, p, w, pi, region, slot_width, my,
-                                       my + 2 * kWfaSeqWords, out, err_flag, work, hist);
-        else
-            wfa_align_pair<U, 1, false>(q, r, p, w, pi, region, slot_width, my,
-                                        my + 2 * kWfaSeqWords, out, err_flag, work, hist);
+        wfa_pair_dispatch<U, 1>(q, r, p, w, pi, region, slot_width, my, my + 2 * kWfaSeqWords,
+                                kWfaSeqWords, out, err_flag, work, hist);
     }
 }
 
