@@ -25,6 +25,8 @@
 // (index k + rlen + 2).  Invariant: inside the interval [GL, GH] that a pair
 // has touched, every slot position outside that slot's own interval holds
 // NEG; so source reads at k-1, k, k+1 need no bounds tests.
+#include <type_traits>
+
 #include "gb2_internal.cuh"
 
 namespace gb2 {
@@ -341,11 +343,14 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                     const RT *Moe = soe >= 0 ? M(soe) : nullptr;
                     const RT *Ie = se >= 0 ? I(se) : nullptr;
                     const RT *De = se >= 0 ? D(se) : nullptr;
-                    for (int32_t k0 = a + tt; k0 <= b; k0 += TW * U) {
-                        int32_t ks[U], iv[U], dv[U], mv[U];
-                        bool live[U];
+                    // rounds of U diagonals per thread while all U are inside
+                    // [a, b], then single-diagonal rounds for the rest
+                    auto round = [&](int32_t k0, auto uc) {
+                        constexpr int UU = decltype(uc)::value;
+                        int32_t ks[UU], iv[UU], dv[UU], mv[UU];
+                        bool live[UU];
 #pragma unroll
-                        for (int u = 0; u < U; ++u) {
+                        for (int u = 0; u < UU; ++u) {
                             ks[u] = k0 + TW * u;
                             live[u] = ks[u] <= b;
                             const int32_t kc = live[u] ? ks[u] : b;  // loads stay in [a-1, b+1]
@@ -365,9 +370,9 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                             const int32_t m1 = max(m0, max(iv[u], d0));
                             mv[u] = m1 < 0 ? NEG : m1;
                         }
-                        extend_u<U, SMEM>(qs, qlen, rs, rlen, mv, ks, live);
+                        extend_u<UU, SMEM>(qs, qlen, rs, rlen, mv, ks, live);
 #pragma unroll
-                        for (int u = 0; u < U; ++u) {
+                        for (int u = 0; u < UU; ++u) {
                             if (live[u]) {
                                 Iw[ks[u]] = (RT)iv[u];
                                 Dw[ks[u]] = (RT)dv[u];
@@ -375,7 +380,12 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                                 hit |= ks[u] == target && mv[u] >= qlen;
                             }
                         }
-                    }
+                    };
+                    int32_t k0 = a + tt;
+                    for (; k0 + TW * (U - 1) <= b; k0 += TW * U)
+                        round(k0, std::integral_constant<int, U>{});
+                    for (; k0 <= b; k0 += TW)
+                        round(k0, std::integral_constant<int, 1>{});
                     // widen for the next step (see above); the positions
                     // filled lie outside everything this step reads or writes
                     if (a - 2 < GL || b + 2 > GH) {
