@@ -202,15 +202,18 @@ struct WfaShape {
 };
 
 // Ring element: int32 (NEG = -2^30) or, when every value a pair can store
-// fits (rows <= qlen + max_error/g <= 32767, checked by the caller), int16
-// (NEG = -16384): half the ring bytes.  Arithmetic is int32 either way and
-// negative results are stored as NEG, so both give the same values.
+// fits, int16 (NEG = -32768): half the ring bytes.  A value gains at most one
+// per score step, so after S = max_error/g steps rows are at most qlen + S and
+// a value that started at NEG is at most NEG + S; the caller takes int16 only
+// when qlen + S <= 32767, where NEG + S <= -1 - qlen stays negative -- so on
+// that path negative values need no renormalisation.  The int32 path stores
+// every negative result as NEG.  Arithmetic is int32 either way.
 template <typename RT> struct RingNeg;
 template <> struct RingNeg<int32_t> {
     static constexpr int32_t value = WFA_NEG;
 };
 template <> struct RingNeg<int16_t> {
-    static constexpr int32_t value = -16384;
+    static constexpr int32_t value = -32768;
 };
 
 template <int U, int TEAM, bool SMEM, typename RT>
@@ -365,10 +368,15 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                             }
                             if (Mx)
                                 m0 = (int32_t)Mx[kc] + 1;
-                            iv[u] = i0 < 0 ? NEG : i0 + 1;
+                            const int32_t m1 = max(m0, max(i0 + 1, d0));
+                            if (std::is_same<RT, int16_t>::value) {
+                                iv[u] = i0 + 1;
+                                mv[u] = m1;
+                            } else {
+                                iv[u] = i0 < 0 ? NEG : i0 + 1;
+                                mv[u] = m1 < 0 ? NEG : m1;
+                            }
                             dv[u] = d0;
-                            const int32_t m1 = max(m0, max(iv[u], d0));
-                            mv[u] = m1 < 0 ? NEG : m1;
                         }
                         extend_u<UU, SMEM>(qs, qlen, rs, rlen, mv, ks, live);
 #pragma unroll
