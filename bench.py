@@ -383,7 +383,7 @@ def our_arm(args, dist: Dist):
     dq.close()
     dr.close()
     if line is not None and dist.world == 1 and not args.no_extras:
-        line["extras"] = extras(args, dev)
+        line["extras"] = extras(args, dev, line["roofline"]["peak"])
     dev.close()
     dist.close()
     if line:
@@ -404,7 +404,7 @@ def _time_steps(dev, fn, steps, warmup):
     return statistics.median(ts)
 
 
-def extras(args, dev):
+def extras(args, dev, peak_ops):
     """Batched queue vs plain launch vs per-call drop-in on the mixed-length workloads,
     with the CPU restatement of the reference beside each (all host threads)."""
     import oracle as O
@@ -484,6 +484,12 @@ def extras(args, dev):
         "cpu_pairs_per_s": round(ns / tcpu, 2), "cpu_cores": threads,
         "cpu_sample": f"first {ns} pairs, statement-for-statement port (per-score reset of "
                       f"2*max_error+1 diagonals, as the reference)",
+        # 13 int ops per wavefront cell: I 3, D 1, M 3, one extend step 6
+        "roofline": {"bound": "latency of dependent ring loads per score step",
+                     "ops_per_cell": 13,
+                     "achieved": round(wcells * 13 / (tb * 1e-3) / 1e9, 1),
+                     "peak": peak_ops, "unit": "Gop/s",
+                     "frac": round(wcells * 13 / (tb * 1e-3) / 1e9 / peak_ops, 4)},
     }
     # WFA with CIGAR traceback: the first 20,000 pairs of the same workload
     nc = 20_000
