@@ -112,13 +112,17 @@ __host__ __device__ inline int64_t wfa_hist_record_bytes(int64_t cell_bytes, int
 }
 
 // CIGAR pass over pairs pairs[0..n) (cost and history cell bytes from the
-// cost pass, history record at arena + arena_off[pair]); run-length CIGAR ops of pair i go to
+// cost pass, history record at arena + arena_off[pair]; the first n_team
+// pairs one per 128-thread block, the rest one per warp; counters[0] and
+// counters[32] zeroed); run-length CIGAR ops of pair i go to
 // runs[run_off[i] ..], their count to run_count[i].  A run is len << 2 | op
 // (op 0 '=', 1 'X', 2 'I', 3 'D').
+// Resident 128-thread blocks per SM of the CIGAR kernel.
+int wfa_cigar_blocks_per_sm();
 cudaError_t launch_wfa_cigar(SeqView q, SeqView r, WfaParams p, const int32_t *pairs, int64_t n,
-                             int *counter, const int32_t *cost, const int64_t *hist_cells,
-                             const int64_t *arena_off, uint8_t *arena, int32_t *scratch,
-                             int64_t slot_width, int grid, uint32_t *runs,
+                             int64_t n_team, int *counters, const int32_t *cost,
+                             const int64_t *hist_cells, const int64_t *arena_off, uint8_t *arena,
+                             int32_t *scratch, int64_t slot_width, int grid, uint32_t *runs,
                              const int64_t *run_off, int32_t *run_count, int *err_flag,
                              cudaStream_t st);
 

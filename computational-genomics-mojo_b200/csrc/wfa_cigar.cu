@@ -1,33 +1,17 @@
-// wfa_cigar.cu -- gap-affine WFA with CIGAR traceback on sm_100a.
+// wfa_cigar.cu -- host side of gap-affine WFA with CIGAR traceback.
 //
 // wfa_affine_cigar_cpu (genomics/cpu/align_cpu.mojo:380-623) keeps M before
 // and after extension, I and D for every score up to the optimum and every
 // diagonal in [-max_err, max_err], then walks back from (opt, qlen - rlen).
 // Here a first pass is the cost kernel, which also reports how many bytes
-// each pair's history will take; a second pass re-runs the forward
-// recurrences (same visited intervals and rings as the cost kernel, one warp
-// per pair) and appends, for every visited score, the M-after-extension
-// values and one decision byte per diagonal to the pair's history record in
-// an arena sized from the first pass.  The decision byte records what the
-// reference's traceback finds by comparing values (:509-601):
-//   * M before extension came from the mismatch source when M[s-x, k] + 1
-//     equals it, else from I when I[s, k] equals it, else from D;
-//   * I[s, k] came from an open when M[s-o-e, k-1] + 1 equals it, else from
-//     an extension I[s-e, k-1] + 1;
-//   * D[s, k] came from an open when M[s-o-e, k+1] equals it, else from
-//     D[s-e, k+1]
-// (the same priority order as the traceback's tests).  With those bytes the
-// traceback needs only M-after values:
-//   M state (s, k), current row = M-after[s, k]: the row before extension is
-//     (mismatch) M-after[s-x, k] + 1; (I) follow the I chain back to its
-//     open (s', k'): M-after[s'-o-e, k'-1] + 1 + number of extensions;
-//     (D) the D chain's open: M-after[s'-o-e, k'+1].  Emit (row - before)
-//     '=' ops, then 'X' and go to (s-x, k), or enter I or D;
-//   I state: one 'I', then M at (s-o-e, k-1) or I at (s-e, k-1);
-//   D state: one 'D', then M at (s-o-e, k+1) or D at (s-e, k+1);
-// ending at score 0, diagonal 0.  Ops come out back to front and are
-// run-length encoded as the reference does (:603-621): a run is
-// len << 2 | op, op 0 '=', 1 'X', 2 'I', 3 'D'.
+// each pair's history record will take; a second pass (wfa_cigar_kernel in
+// wfa_kernels.cu) re-runs each pair's forward recurrences with the cost
+// kernel's own code in history mode, appending per visited score the
+// M-after-extension values and one decision byte per diagonal to the pair's
+// record in an arena sized from the first pass, and walks the record back
+// into CIGAR runs (wfa_trace.cuh).  The host groups pairs, largest records
+// first, so the records of a group fit the arena, then gathers every pair's
+// runs into the caller's array.
 //
 // A history record costs 4 B + 1 B per visited cell plus 12 B per score,
 // against the reference's 4 int64 arrays over (max_err+1) x (2 max_err+1).
@@ -39,445 +23,7 @@
 #include "runtime.cuh"
 
 namespace gb2 {
-
-#define WFA_NEG_C (-(1 << 30))
-
 namespace {
-
-__device__ __forceinline__ int gcd_c(int a, int b)
-{
-    while (b) {
-        int t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
-struct Halves {
-    const uint32_t *w;
-    int32_t last;
-    uint32_t swz;
-};
-
-// 16 bases at pos (see the cost kernel's window16: halves high first in
-// shared memory, swz = 1 for the little-endian words in global memory).
-__device__ __forceinline__ uint32_t win16(const Halves &s, int32_t pos)
-{
-    const int32_t j = pos >> 4;
-    const uint32_t hi = s.w[(uint32_t)j ^ s.swz];
-    const uint32_t lo = s.w[(uint32_t)min(j + 1, s.last) ^ s.swz];
-    return __funnelshift_l(lo, hi, (uint32_t)(pos & 15) << 1);
-}
-
-// Extend along diagonal k from row (align_cpu.mojo:489-498).
-__device__ __forceinline__ int32_t extend16(const Halves &qs, int32_t qlen, const Halves &rs,
-                                            int32_t rlen, int32_t row, int32_t k)
-{
-    if (row < 0 || row - k < 0)
-        return row;
-    int32_t col = row - k;
-    while (row < qlen && col < rlen) {
-        const uint32_t x = win16(qs, row) ^ win16(rs, col);
-        const int ml = x ? (__clz((int)x) >> 1) : 16;
-        const int lim = min(qlen - row, rlen - col);
-        if (ml >= lim)
-            return row + lim;
-        row += ml;
-        col += ml;
-        if (ml < 16)
-            break;
-    }
-    return row;
-}
-
-constexpr int kSeqWords = 321;  // per sequence per warp: 10,240 bases + a zero pad
-
-__device__ __forceinline__ Halves stage(const SeqView &v, int64_t off, int32_t nw, uint32_t *smem,
-                                        int lane)
-{
-    if (nw < kSeqWords) {
-        uint2 *d = reinterpret_cast<uint2 *>(smem);
-        for (int i = lane; i <= nw; i += 32) {
-            const uint64_t x = i < nw ? __ldg(v.packed + off + i) : 0;
-            d[i] = make_uint2((uint32_t)(x >> 32), (uint32_t)x);
-        }
-        return Halves{smem, 2 * nw, 0u};
-    }
-    const int64_t last = 2 * (v.n_words - off) - 1;
-    return Halves{reinterpret_cast<const uint32_t *>(v.packed + off),
-                  (int32_t)min(last, (int64_t)0x7fffffff), 1u};
-}
-
-// Read access to one pair's history record.
-struct Hist {
-    const uint8_t *rec;
-    const int32_t *hdr;
-    __device__ __forceinline__ int32_t mafter(int sp, int32_t k) const
-    {
-        if (sp < 0)
-            return WFA_NEG_C;
-        const int32_t a = hdr[3 * sp], b = hdr[3 * sp + 1];
-        if (k < a || k > b)
-            return WFA_NEG_C;
-        return reinterpret_cast<const int32_t *>(rec)[hdr[3 * sp + 2] + (k - a)];
-    }
-    __device__ __forceinline__ uint32_t dec(int sp, int32_t k) const
-    {
-        if (sp < 0)
-            return 0;
-        const int32_t a = hdr[3 * sp], b = hdr[3 * sp + 1];
-        if (k < a || k > b)
-            return 0;
-        const int64_t off = hdr[3 * sp + 2];
-        return rec[(off + (b - a + 1)) * 4 + (k - a)];
-    }
-};
-
-__global__ void __launch_bounds__(128)
-wfa_cigar_kernel(SeqView q, SeqView r, WfaParams p, const int32_t *__restrict__ pairs, int64_t n,
-                 int *counter, const int32_t *__restrict__ cost,
-                 const int64_t *__restrict__ hist_cells, const int64_t *__restrict__ arena_off,
-                 uint8_t *__restrict__ arena, int32_t *__restrict__ scratch, int64_t slot_width,
-                 uint32_t *__restrict__ runs, const int64_t *__restrict__ run_off,
-                 int32_t *__restrict__ run_count, int *err_flag)
-{
-    __shared__ __align__(16) uint32_t seqs[4 * 2 * 2 * kSeqWords];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int g = gcd_c(p.x, gcd_c(p.o, p.e));
-    const int xs = p.x / g, oes = (p.o + p.e) / g, es = p.e / g;
-    const int hm = max(xs, oes) + 1, hie = es + 1;
-    const int nslot = hm + 2 * hie;
-    int32_t *const region = scratch + ((int64_t)blockIdx.x * 4 + wib) * nslot * slot_width;
-    uint32_t *const my = seqs + wib * 4 * kSeqWords;
-
-    for (;;) {
-        int64_t b0 = 0;
-        if (lane == 0)
-            b0 = atomicAdd(counter, 1);
-        const int64_t si = __shfl_sync(FULL, b0, 0);
-        if (si >= n)
-            break;
-        const int64_t pi = pairs[si];
-        const int32_t c = cost[pi];
-        const int64_t qoff = q.offsets[pi] - q.word_base;
-        const int64_t roff = r.offsets[pi] - r.word_base;
-        const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
-        if (c < 0 || (qlen == 0 && rlen == 0)) {
-            if (lane == 0)
-                run_count[pi] = 0;
-            continue;
-        }
-        if ((int64_t)qlen + rlen + 5 > slot_width || c % g != 0) {
-            if (lane == 0) {
-                atomicOr(err_flag, 1);
-                run_count[pi] = -1;
-            }
-            continue;
-        }
-        const int S = c / g + 1;  // visited score indices 0 .. c/g
-        uint8_t *const rec = arena + arena_off[pi];
-        int32_t *const hdr = reinterpret_cast<int32_t *>(rec);
-        int32_t *const recw = reinterpret_cast<int32_t *>(rec);
-        int64_t cur = 3 * (int64_t)S;  // next free 4-byte word of the record
-        // the record's size from the cost pass; a step that would pass it
-        // (the two passes disagree) stops the pair with an error instead
-        const int64_t limit = cur + hist_cells[pi] / 4;
-        bool overrun = false;
-
-        __syncwarp();  // the previous pair's reads of the shared copies are done
-        const Halves qs = stage(q, qoff, (qlen + 31) >> 5, my, lane);
-        const Halves rs = stage(r, roff, (rlen + 31) >> 5, my + 2 * kSeqWords, lane);
-        const int32_t kofs = rlen + 2;
-        const int32_t target = qlen - rlen;
-        int32_t *const base = region + kofs;
-        auto M = [&](int slot) { return base + (int64_t)slot * slot_width; };
-        auto I = [&](int slot) { return base + (int64_t)(hm + slot) * slot_width; };
-        auto D = [&](int slot) { return base + (int64_t)(hm + hie + slot) * slot_width; };
-        int32_t mlo = 1, mhi = 0, ilo = 1, ihi = 0;
-        int32_t GL = max(-2, -rlen - 2), GH = min(2, qlen + 2);
-        for (int sl = 0; sl < nslot; ++sl) {
-            int32_t *row = base + (int64_t)sl * slot_width;
-            for (int32_t k = GL + lane; k <= GH; k += 32)
-                row[k] = WFA_NEG_C;
-        }
-        __syncwarp();
-        const int32_t row0 = extend16(qs, qlen, rs, rlen, 0, 0);
-        if (lane == 0) {  // score 0 (cur + 2 <= limit: the cost pass counts 8 bytes for it)
-            mlo = 0;
-            mhi = 0;
-            M(0)[0] = row0;
-            hdr[0] = 0;
-            hdr[1] = 0;
-            hdr[2] = (int32_t)cur;
-            recw[cur] = row0;
-            rec[(cur + 1) * 4] = 0;
-        }
-        cur += wfa_hist_cell_bytes(1) / 4;
-        __syncwarp();
-        int32_t result = (target == 0 && row0 >= qlen) ? 0 : -1;
-        int ms = 0, is = 0;
-        for (int sp = 1; result < 0 && sp < S; ++sp) {
-            const int32_t s = sp * g;
-            ms = ms + 1 == hm ? 0 : ms + 1;
-            is = is + 1 == hie ? 0 : is + 1;
-            int32_t lo = max(-rlen, -s), hi = min(qlen, s);
-            if (target < lo || target > hi) {
-                lo = min(lo, target);
-                hi = max(hi, target);
-            }
-            lo = max(lo, -p.max_error);
-            hi = min(hi, p.max_error);
-            const int sx = sp >= xs ? (ms >= xs ? ms - xs : ms - xs + hm) : -1;
-            const int soe = sp >= oes ? (ms >= oes ? ms - oes : ms - oes + hm) : -1;
-            const int se = sp >= es ? (is >= es ? is - es : is - es + hie) : -1;
-            int32_t ulo = 0x7fffffff, uhi = -0x7fffffff;
-            {
-                const int32_t a0 = __shfl_sync(FULL, mlo, sx & 31);
-                const int32_t b0v = __shfl_sync(FULL, mhi, sx & 31);
-                if (sx >= 0 && a0 <= b0v) {
-                    ulo = a0;
-                    uhi = b0v;
-                }
-                const int32_t a1 = __shfl_sync(FULL, mlo, soe & 31);
-                const int32_t b1 = __shfl_sync(FULL, mhi, soe & 31);
-                if (soe >= 0 && a1 <= b1) {
-                    ulo = min(ulo, a1 - 1);
-                    uhi = max(uhi, b1 + 1);
-                }
-                const int32_t a2 = __shfl_sync(FULL, ilo, se & 31);
-                const int32_t b2 = __shfl_sync(FULL, ihi, se & 31);
-                if (se >= 0 && a2 <= b2) {
-                    ulo = min(ulo, a2 - 1);
-                    uhi = max(uhi, b2 + 1);
-                }
-            }
-            const int32_t a = max(ulo, lo);
-            const int32_t b = min(uhi, hi);
-            const int32_t omlo = __shfl_sync(FULL, mlo, ms);
-            const int32_t omhi = __shfl_sync(FULL, mhi, ms);
-            const int32_t oilo = __shfl_sync(FULL, ilo, is);
-            const int32_t oihi = __shfl_sync(FULL, ihi, is);
-            int32_t *const Mw = M(ms), *const Iw = I(is), *const Dw = D(is);
-            const int32_t ca = a > b ? 0x7fffffff : a, cb = a > b ? -0x7fffffff : b;
-            for (int32_t k = omlo + lane; k <= min(omhi, ca - 1); k += 32)
-                Mw[k] = WFA_NEG_C;
-            for (int32_t k = max(omlo, cb + 1) + lane; k <= omhi; k += 32)
-                Mw[k] = WFA_NEG_C;
-            for (int32_t k = oilo + lane; k <= min(oihi, ca - 1); k += 32) {
-                Iw[k] = WFA_NEG_C;
-                Dw[k] = WFA_NEG_C;
-            }
-            for (int32_t k = max(oilo, cb + 1) + lane; k <= oihi; k += 32) {
-                Iw[k] = WFA_NEG_C;
-                Dw[k] = WFA_NEG_C;
-            }
-            if (lane == 0) {
-                hdr[3 * sp] = a <= b ? a : 1;
-                hdr[3 * sp + 1] = a <= b ? b : 0;
-                hdr[3 * sp + 2] = a <= b ? (int32_t)cur : 0;
-            }
-            bool hit = false;
-            if (a <= b && cur + wfa_hist_cell_bytes(b - a + 1) / 4 > limit) {
-                overrun = true;  // same decision in every lane
-                break;
-            }
-            if (a <= b) {
-                const int32_t wdt = b - a + 1;
-                int32_t *const hm_out = recw + cur;
-                uint8_t *const hd_out = rec + (cur + wdt) * 4;
-                const int32_t *Mx = sx >= 0 ? M(sx) : nullptr;
-                const int32_t *Moe = soe >= 0 ? M(soe) : nullptr;
-                const int32_t *Ie = se >= 0 ? I(se) : nullptr;
-                const int32_t *De = se >= 0 ? D(se) : nullptr;
-                for (int32_t k = a + lane; k <= b; k += 32) {
-                    int32_t io = WFA_NEG_C, ie = WFA_NEG_C, dop = WFA_NEG_C, dex = WFA_NEG_C,
-                            mx = WFA_NEG_C;
-                    if (Moe) {
-                        io = Moe[k - 1];
-                        dop = Moe[k + 1];
-                    }
-                    if (Ie) {
-                        ie = Ie[k - 1];
-                        dex = De[k + 1];
-                    }
-                    if (Mx)
-                        mx = Mx[k];
-                    const int32_t io1 = io < 0 ? WFA_NEG_C : io + 1;
-                    const int32_t ie1 = ie < 0 ? WFA_NEG_C : ie + 1;
-                    const int32_t iv = max(io1, ie1);
-                    const int32_t dv = max(dop < 0 ? WFA_NEG_C : dop, dex < 0 ? WFA_NEG_C : dex);
-                    const int32_t mx1 = mx < 0 ? WFA_NEG_C : mx + 1;
-                    const int32_t mpre = max(mx1, max(iv, dv));
-                    uint32_t dec = 0;
-                    if (mpre >= 0)
-                        dec = (mx1 >= 0 && mx1 == mpre) ? 1u : ((iv >= 0 && iv == mpre) ? 2u : 3u);
-                    if (iv >= 0 && !(io1 >= 0 && io1 == iv))
-                        dec |= 4u;
-                    if (dv >= 0 && !(dop >= 0 && dop == dv))
-                        dec |= 8u;
-                    const int32_t mv =
-                        mpre >= 0 ? extend16(qs, qlen, rs, rlen, mpre, k) : WFA_NEG_C;
-                    Iw[k] = iv;
-                    Dw[k] = dv;
-                    Mw[k] = mv;
-                    hm_out[k - a] = mv;
-                    hd_out[k - a] = (uint8_t)dec;
-                    hit |= k == target && mv >= qlen;
-                }
-                cur += wfa_hist_cell_bytes(wdt) / 4;
-                if (a - 2 < GL || b + 2 > GH) {
-                    const int32_t nGL = a - 2 < GL ? max(a - 2 - 30, -rlen - 2) : GL;
-                    const int32_t nGH = b + 2 > GH ? min(b + 2 + 30, qlen + 2) : GH;
-                    for (int sl = 0; sl < nslot; ++sl) {
-                        int32_t *rowp = base + (int64_t)sl * slot_width;
-                        for (int32_t k = nGL + lane; k < GL; k += 32)
-                            rowp[k] = WFA_NEG_C;
-                        for (int32_t k = GH + 1 + lane; k <= nGH; k += 32)
-                            rowp[k] = WFA_NEG_C;
-                    }
-                    GL = nGL;
-                    GH = nGH;
-                }
-            }
-            if (lane == ms) {
-                mlo = a <= b ? a : 1;
-                mhi = a <= b ? b : 0;
-            }
-            if (lane == is) {
-                ilo = a <= b ? a : 1;
-                ihi = a <= b ? b : 0;
-            }
-            __syncwarp();
-            if (__any_sync(FULL, hit))
-                result = s;
-        }
-        __syncwarp();  // the record is complete and visible to lane 0
-        if (lane != 0)
-            continue;
-        if (overrun || result != c) {  // the cost pass and this pass disagree
-            atomicOr(err_flag, 2);
-            run_count[pi] = -1;
-            continue;
-        }
-        // traceback by lane 0 (ops back to front, merged into runs)
-        const Hist h{rec, hdr};
-        uint32_t *const dst = runs + run_off[pi];
-        const int64_t cap = (int64_t)qlen + rlen + 1;
-        int64_t nrun = 0;
-        uint32_t cur_op = 4, cur_len = 0;
-        bool bad = false;
-        auto emit = [&](uint32_t op, int32_t cnt) {
-            if (cnt <= 0)
-                return;
-            if (op == cur_op) {
-                cur_len += (uint32_t)cnt;
-                return;
-            }
-            if (cur_len) {
-                if (nrun >= cap) {
-                    bad = true;
-                    return;
-                }
-                dst[nrun++] = cur_len << 2 | cur_op;
-            }
-            cur_op = op;
-            cur_len = (uint32_t)cnt;
-        };
-        int sp = c / g, mode = 0;
-        int32_t k = target, crow = h.mafter(sp, k);
-        for (int64_t guard = 4 * ((int64_t)qlen + rlen) + 16; !bad; --guard) {
-            if (guard <= 0 || sp < 0) {
-                bad = true;
-                break;
-            }
-            if (mode == 0) {
-                const uint32_t src = h.dec(sp, k) & 3u;
-                int32_t before;
-                if (sp == 0) {
-                    before = 0;  // M[0, 0] = 0 before extension
-                } else if (src == 1) {
-                    before = h.mafter(sp - xs, k) + 1;
-                } else if (src == 2) {
-                    int ssp = sp, j = 0;
-                    int32_t kk = k;
-                    while (ssp >= 0 && (h.dec(ssp, kk) & 4u)) {
-                        ssp -= es;
-                        kk -= 1;
-                        ++j;
-                    }
-                    before = h.mafter(ssp - oes, kk - 1) + 1 + j;
-                } else if (src == 3) {
-                    int ssp = sp;
-                    int32_t kk = k;
-                    while (ssp >= 0 && (h.dec(ssp, kk) & 8u)) {
-                        ssp -= es;
-                        kk += 1;
-                    }
-                    before = h.mafter(ssp - oes, kk + 1);
-                } else {
-                    bad = true;
-                    break;
-                }
-                emit(0, crow - before);
-                crow = before;
-                if (sp == 0) {
-                    if (k != 0)
-                        bad = true;
-                    break;
-                }
-                if (src == 1) {
-                    emit(1, 1);
-                    sp -= xs;
-                    crow = h.mafter(sp, k);
-                } else {
-                    mode = (int)src - 1;  // 1: I, 2: D
-                }
-            } else if (mode == 1) {
-                emit(2, 1);
-                if (h.dec(sp, k) & 4u) {
-                    sp -= es;
-                    k -= 1;
-                    crow -= 1;
-                } else {
-                    sp -= oes;
-                    k -= 1;
-                    crow = h.mafter(sp, k);
-                    mode = 0;
-                }
-            } else {
-                emit(3, 1);
-                if (h.dec(sp, k) & 8u) {
-                    sp -= es;
-                    k += 1;
-                } else {
-                    sp -= oes;
-                    k += 1;
-                    crow = h.mafter(sp, k);
-                    mode = 0;
-                }
-            }
-        }
-        if (!bad && cur_len) {
-            if (nrun >= cap)
-                bad = true;
-            else
-                dst[nrun++] = cur_len << 2 | cur_op;
-        }
-        if (bad) {
-            atomicOr(err_flag, 4);
-            run_count[pi] = -1;
-            continue;
-        }
-        for (int64_t i = 0, j = nrun - 1; i < j; ++i, --j) {
-            const uint32_t t = dst[i];
-            dst[i] = dst[j];
-            dst[j] = t;
-        }
-        run_count[pi] = (int32_t)nrun;
-    }
-}
 
 // Gathers every pair's runs into one contiguous array (warp per pair).
 __global__ void k_compact_runs(int64_t n, const uint32_t *__restrict__ runs,
@@ -496,32 +42,6 @@ __global__ void k_compact_runs(int64_t n, const uint32_t *__restrict__ runs,
 }
 
 }  // namespace
-
-cudaError_t launch_wfa_cigar(SeqView q, SeqView r, WfaParams p, const int32_t *pairs, int64_t n,
-                             int *counter, const int32_t *cost, const int64_t *hist_cells,
-                             const int64_t *arena_off, uint8_t *arena, int32_t *scratch,
-                             int64_t slot_width, int grid, uint32_t *runs,
-                             const int64_t *run_off, int32_t *run_count, int *err_flag,
-                             cudaStream_t st)
-{
-    if (n <= 0)
-        return cudaSuccess;
-    wfa_cigar_kernel<<<grid, 128, 0, st>>>(q, r, p, pairs, n, counter, cost, hist_cells,
-                                           arena_off, arena, scratch, slot_width, runs, run_off,
-                                           run_count, err_flag);
-    return cudaGetLastError();
-}
-
-static int cigar_blocks_per_sm()
-{
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_cigar_kernel, 128, 0) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        return 4;
-    }
-    return std::max(nb, 1);
-}
 
 }  // namespace gb2
 
@@ -585,7 +105,7 @@ static int wfa_cigar_run(gb2_ctx *c, SeqView qv, SeqView rv, const int64_t *h_ql
     const int nslot = hm + 2 * hie;
     const int64_t slot_width = ((qmax + rmax + 5) + 31) & ~int64_t(31);
     const int64_t warp_bytes = (int64_t)nslot * slot_width * 4;
-    int64_t grid = (int64_t)c->sm_count * cigar_blocks_per_sm();
+    int64_t grid = (int64_t)c->sm_count * wfa_cigar_blocks_per_sm();
     grid = std::min(grid, std::max<int64_t>(c->sm_count, kWfaScratchCap / (4 * warp_bytes)));
     grid = std::min(grid, std::max<int64_t>(1, (n + 3) / 4));
     // the arena: the budget, or all records when they fit in less
@@ -624,13 +144,15 @@ static int wfa_cigar_run(gb2_ctx *c, SeqView qv, SeqView rv, const int64_t *h_ql
                                   cudaMemcpyHostToDevice, x.st));
         GB2_CU(c, cudaMemcpyAsync(cb.arena_off.p, aoff.data(), (size_t)n * 8,
                                   cudaMemcpyHostToDevice, x.st));
-        GB2_CU(c, cudaMemsetAsync(x.counters.p, 0, 64, x.st));
-        GB2_CU(c, launch_wfa_cigar(qv, rv, p, (const int32_t *)cb.pairs.p, m,
+        // the largest records of the group, one wave of blocks, one pair per block
+        const int gg = (int)std::min<int64_t>(grid, (m + 3) / 4);
+        const int64_t n_team = std::min<int64_t>(gg, m);
+        GB2_CU(c, cudaMemsetAsync(x.counters.p, 0, 256, x.st));
+        GB2_CU(c, launch_wfa_cigar(qv, rv, p, (const int32_t *)cb.pairs.p, m, n_team,
                                    (int *)x.counters.p, (const int32_t *)cb.cost.p,
                                    (const int64_t *)cb.hist.p,
                                    (const int64_t *)cb.arena_off.p, (uint8_t *)cb.arena.p,
-                                   (int32_t *)x.scratch32.p, slot_width,
-                                   (int)std::min<int64_t>(grid, (m + 3) / 4),
+                                   (int32_t *)x.scratch32.p, slot_width, gg,
                                    (uint32_t *)cb.runs.p, (const int64_t *)cb.run_off.p,
                                    (int32_t *)cb.run_count.p, (int *)x.errflag.p, x.st));
         c->launches += 1;

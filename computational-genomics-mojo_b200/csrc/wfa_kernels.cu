@@ -28,6 +28,7 @@
 #include <type_traits>
 
 #include "gb2_internal.cuh"
+#include "wfa_trace.cuh"
 
 namespace gb2 {
 
@@ -216,13 +217,18 @@ template <> struct RingNeg<int16_t> {
     static constexpr int32_t value = -32768;
 };
 
-template <int U, int TEAM, bool SMEM, typename RT>
-__device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &r,
-                                               const WfaParams &p, const WfaShape &w,
-                                               int64_t pi, int32_t *region, int64_t slot_width,
-                                               uint32_t *sq, uint32_t *sr,
-                                               int32_t *__restrict__ out, int *err_flag,
-                                               int64_t *work, int64_t *hist)
+// HREC: also write the pair's history record (the CIGAR pass): at most
+// hsteps score indices (the cost is known), into hrec, whose cell part ends
+// at 4-byte word hlimit; a step that would pass it makes the call return -3.
+// Returns the cost (team-uniform).
+template <int U, int TEAM, bool SMEM, typename RT, bool HREC>
+__device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqView &r,
+                                                  const WfaParams &p, const WfaShape &w,
+                                                  int64_t pi, int32_t *region, int64_t slot_width,
+                                                  uint32_t *sq, uint32_t *sr,
+                                                  int32_t *__restrict__ out, int *err_flag,
+                                                  int64_t *work, int64_t *hist, uint8_t *hrec,
+                                                  int64_t hlimit, int hsteps)
 {
     constexpr int TW = TEAM * 32;
     constexpr int32_t NEG = RingNeg<RT>::value;
@@ -237,6 +243,9 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
     int32_t result = -1;
     int64_t cells = 0;
     int64_t hbytes = 8;  // history bytes of the visited cells (score 0: one cell)
+    int32_t *const hdr = reinterpret_cast<int32_t *>(hrec);
+    int64_t hcur = 3 * (int64_t)hsteps;  // next free 4-byte word of the record
+    bool overrun = false;
     if (qlen == 0 && rlen == 0) {
         result = 0;
     } else if ((int64_t)qlen + rlen + 5 > slot_width) {
@@ -273,12 +282,22 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         }
         if (tt == 0)
             M(0)[0] = (RT)row0;
+        if (HREC) {
+            if (tt == 0) {
+                hdr[0] = 0;
+                hdr[1] = 0;
+                hdr[2] = (int32_t)hcur;
+                hdr[hcur] = row0;
+                hrec[(hcur + 1) * 4] = 0;
+            }
+            hcur += wfa_hist_cell_bytes(1) / 4;
+        }
         team_sync<TEAM>();
         if (target == 0 && row0 >= qlen) {
             result = 0;
         } else {
             int ms = 0, is = 0;  // ring slots of the current score
-            for (int64_t sp = 1; sp * g <= max_err; ++sp) {
+            for (int64_t sp = 1; HREC ? sp < hsteps : sp * g <= max_err; ++sp) {
                 const int32_t s = (int32_t)(sp * g);
                 ms = ms + 1 == hm ? 0 : ms + 1;
                 is = is + 1 == hie ? 0 : is + 1;
@@ -338,6 +357,21 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                         Dw[k] = NEG;
                     }
                 }
+                int32_t *hm_out = nullptr;  // this score's part of the record
+                uint8_t *hd_out = nullptr;
+                if (HREC) {
+                    if (a <= b && hcur + wfa_hist_cell_bytes(b - a + 1) / 4 > hlimit) {
+                        overrun = true;  // same decision in every thread
+                        break;
+                    }
+                    if (tt == 0) {
+                        hdr[3 * sp] = a <= b ? a : 1;
+                        hdr[3 * sp + 1] = a <= b ? b : 0;
+                        hdr[3 * sp + 2] = a <= b ? (int32_t)hcur : 0;
+                    }
+                    hm_out = hdr + hcur;
+                    hd_out = hrec + (hcur + (b - a + 1)) * 4;
+                }
                 bool hit = false;
                 if (a <= b) {
                     cells += (int64_t)(b - a + 1);
@@ -351,24 +385,40 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                     auto round = [&](int32_t k0, auto uc) {
                         constexpr int UU = decltype(uc)::value;
                         int32_t ks[UU], iv[UU], dv[UU], mv[UU];
+                        uint32_t dec[UU];
                         bool live[UU];
 #pragma unroll
                         for (int u = 0; u < UU; ++u) {
                             ks[u] = k0 + TW * u;
                             live[u] = ks[u] <= b;
                             const int32_t kc = live[u] ? ks[u] : b;  // loads stay in [a-1, b+1]
-                            int32_t i0 = NEG, d0 = NEG, m0 = NEG;
+                            int32_t io = NEG, ie = NEG, dop = NEG, dex = NEG, mx = NEG;
                             if (Moe) {
-                                i0 = (int32_t)Moe[kc - 1];
-                                d0 = (int32_t)Moe[kc + 1];
+                                io = (int32_t)Moe[kc - 1];
+                                dop = (int32_t)Moe[kc + 1];
                             }
                             if (Ie) {
-                                i0 = max(i0, (int32_t)Ie[kc - 1]);
-                                d0 = max(d0, (int32_t)De[kc + 1]);
+                                ie = (int32_t)Ie[kc - 1];
+                                dex = (int32_t)De[kc + 1];
                             }
                             if (Mx)
-                                m0 = (int32_t)Mx[kc] + 1;
+                                mx = (int32_t)Mx[kc];
+                            const int32_t i0 = max(io, ie), d0 = max(dop, dex), m0 = mx + 1;
                             const int32_t m1 = max(m0, max(i0 + 1, d0));
+                            if (HREC) {
+                                // the traceback's tests (align_cpu.mojo:509-601), first
+                                // equal source: M from mismatch, I, D; I / D from an
+                                // open before an extension
+                                uint32_t d = 0;
+                                if (m1 >= 0)
+                                    d = (mx >= 0 && m0 == m1) ? 1u
+                                                              : ((i0 >= 0 && i0 + 1 == m1) ? 2u : 3u);
+                                if (i0 >= 0 && !(io >= 0 && io == i0))
+                                    d |= 4u;
+                                if (d0 >= 0 && !(dop >= 0 && dop == d0))
+                                    d |= 8u;
+                                dec[u] = d;
+                            }
                             if (std::is_same<RT, int16_t>::value) {
                                 iv[u] = i0 + 1;
                                 mv[u] = m1;
@@ -385,6 +435,10 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                                 Iw[ks[u]] = (RT)iv[u];
                                 Dw[ks[u]] = (RT)dv[u];
                                 Mw[ks[u]] = (RT)mv[u];
+                                if (HREC) {
+                                    hm_out[ks[u] - a] = mv[u];
+                                    hd_out[ks[u] - a] = (uint8_t)dec[u];
+                                }
                                 hit |= ks[u] == target && mv[u] >= qlen;
                             }
                         }
@@ -394,6 +448,8 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
                         round(k0, std::integral_constant<int, U>{});
                     for (; k0 <= b; k0 += TW)
                         round(k0, std::integral_constant<int, 1>{});
+                    if (HREC)
+                        hcur += wfa_hist_cell_bytes(b - a + 1) / 4;
                     // widen for the next step (see above); the positions
                     // filled lie outside everything this step reads or writes
                     if (a - 2 < GL || b + 2 > GH) {
@@ -428,39 +484,46 @@ __device__ __forceinline__ void wfa_align_pair(const SeqView &q, const SeqView &
         }
     }
     if (tt == 0) {
-        out[pi] = result;
+        if (out)
+            out[pi] = result;
         if (work)
             atomicAdd((unsigned long long *)work, (unsigned long long)cells);
         if (hist)
             hist[pi] = result >= 0 ? hbytes : 0;
     }
+    return overrun ? -3 : result;
 }
 
 // Runs pair pi with the shared-memory copies when both sequences fit seqw
 // words (with the pad) and with int16 rings when its rows fit them.
-template <int U, int TEAM>
-__device__ __forceinline__ void wfa_pair_dispatch(const SeqView &q, const SeqView &r,
-                                                  const WfaParams &p, const WfaShape &w,
-                                                  int64_t pi, int32_t *region,
-                                                  int64_t slot_width, uint32_t *sq,
-                                                  uint32_t *sr, int seqw, int32_t *out,
-                                                  int *err_flag, int64_t *work, int64_t *hist)
+template <int U, int TEAM, bool HREC = false>
+__device__ __forceinline__ int32_t wfa_pair_dispatch(const SeqView &q, const SeqView &r,
+                                                     const WfaParams &p, const WfaShape &w,
+                                                     int64_t pi, int32_t *region,
+                                                     int64_t slot_width, uint32_t *sq,
+                                                     uint32_t *sr, int seqw, int32_t *out,
+                                                     int *err_flag, int64_t *work, int64_t *hist,
+                                                     uint8_t *hrec = nullptr, int64_t hlimit = 0,
+                                                     int hsteps = 0)
 {
     const int64_t ql = q.lengths[pi], rl = r.lengths[pi];
     const bool smem = ((ql + 31) >> 5) < seqw && ((rl + 31) >> 5) < seqw;
     const bool r16 = ql + p.max_error / w.g <= 32767;
     if (smem && r16)
-        wfa_align_pair<U, TEAM, true, int16_t>(q, r, p, w, pi, region, slot_width, sq, sr, out,
-                                               err_flag, work, hist);
-    else if (smem)
-        wfa_align_pair<U, TEAM, true, int32_t>(q, r, p, w, pi, region, slot_width, sq, sr, out,
-                                               err_flag, work, hist);
-    else if (r16)
-        wfa_align_pair<U, TEAM, false, int16_t>(q, r, p, w, pi, region, slot_width, sq, sr,
-                                                out, err_flag, work, hist);
-    else
-        wfa_align_pair<U, TEAM, false, int32_t>(q, r, p, w, pi, region, slot_width, sq, sr,
-                                                out, err_flag, work, hist);
+        return wfa_align_pair<U, TEAM, true, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                            sq, sr, out, err_flag, work, hist,
+                                                            hrec, hlimit, hsteps);
+    if (smem)
+        return wfa_align_pair<U, TEAM, true, int32_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                            sq, sr, out, err_flag, work, hist,
+                                                            hrec, hlimit, hsteps);
+    if (r16)
+        return wfa_align_pair<U, TEAM, false, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                             sq, sr, out, err_flag, work, hist,
+                                                             hrec, hlimit, hsteps);
+    return wfa_align_pair<U, TEAM, false, int32_t, HREC>(q, r, p, w, pi, region, slot_width, sq,
+                                                         sr, out, err_flag, work, hist, hrec,
+                                                         hlimit, hsteps);
 }
 
 // Persistent kernel over two length-sorted queues: every block first takes
@@ -523,6 +586,137 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
         wfa_pair_dispatch<U, 1>(q, r, p, w, pi, region, slot_width, my, my + 2 * kWfaSeqWords,
                                 kWfaSeqWords, out, err_flag, work, hist);
     }
+}
+
+// CIGAR pass (see wfa_cigar.cu): re-runs the forward pass of pairs whose cost
+// is known with wfa_align_pair in history mode, then one thread walks the
+// record back into runs.  The first n_team pairs of the list (the largest
+// records) are taken one per block by its 4 warps, the rest one per warp, as
+// in wfa_kernel.
+template <int TEAM>
+__device__ __forceinline__ void cigar_pair(const SeqView &q, const SeqView &r, const WfaParams &p,
+                                           const WfaShape &w, int64_t pi, int32_t *region,
+                                           int64_t slot_width, uint32_t *sq, uint32_t *sr,
+                                           int seqw, const int32_t *cost,
+                                           const int64_t *hist_cells, const int64_t *arena_off,
+                                           uint8_t *arena, uint32_t *runs,
+                                           const int64_t *run_off, int32_t *run_count,
+                                           int *err_flag)
+{
+    const int tt = TEAM == 1 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+    const int32_t c = cost[pi];
+    const int64_t qlen = q.lengths[pi], rlen = r.lengths[pi];
+    if (c < 0 || (qlen == 0 && rlen == 0)) {
+        if (tt == 0)
+            run_count[pi] = 0;
+        return;
+    }
+    if (qlen + rlen + 5 > slot_width || c % w.g != 0) {
+        if (tt == 0) {
+            atomicOr(err_flag, 1);
+            run_count[pi] = -1;
+        }
+        return;
+    }
+    const int S = c / w.g + 1;
+    uint8_t *const rec = arena + arena_off[pi];
+    const int64_t limit = 3 * (int64_t)S + hist_cells[pi] / 4;
+    const int32_t res = wfa_pair_dispatch<4, TEAM, true>(q, r, p, w, pi, region, slot_width, sq,
+                                                         sr, seqw, nullptr, err_flag, nullptr,
+                                                         nullptr, rec, limit, S);
+    team_sync<TEAM>();  // the record is complete and visible to thread 0
+    if (tt != 0)
+        return;
+    if (res != c) {  // the cost pass and this pass disagree
+        atomicOr(err_flag, 2);
+        run_count[pi] = -1;
+        return;
+    }
+    const int64_t nrun = wfa_traceback(rec, c, w.g, w.xs, w.oes, w.es, (int32_t)qlen,
+                                       (int32_t)rlen, runs + run_off[pi], qlen + rlen + 1);
+    if (nrun < 0) {
+        atomicOr(err_flag, 4);
+        run_count[pi] = -1;
+    } else {
+        run_count[pi] = (int32_t)nrun;
+    }
+}
+
+__global__ void __launch_bounds__(128)
+wfa_cigar_kernel(SeqView q, SeqView r, WfaParams p, const int32_t *__restrict__ pairs, int64_t n,
+                 int64_t n_team, int *counters, const int32_t *__restrict__ cost,
+                 const int64_t *__restrict__ hist_cells, const int64_t *__restrict__ arena_off,
+                 uint8_t *__restrict__ arena, int32_t *__restrict__ scratch, int64_t slot_width,
+                 uint32_t *__restrict__ runs, const int64_t *__restrict__ run_off,
+                 int32_t *__restrict__ run_count, int *err_flag)
+{
+    __shared__ __align__(16) uint32_t seqs[4 * 2 * 2 * kWfaSeqWords];
+    __shared__ int64_t team_slot;
+    WfaShape w;
+    w.g = gcd_i(p.x, gcd_i(p.o, p.e));
+    w.xs = p.x / w.g;
+    w.oes = (p.o + p.e) / w.g;
+    w.es = p.e / w.g;
+    w.hm = max(w.xs, w.oes) + 1;
+    w.hie = w.es + 1;
+    w.nslot = w.hm + 2 * w.hie;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t region_words = (int64_t)w.nslot * slot_width;
+    if (n_team > 0) {
+        int32_t *const region = scratch + (int64_t)blockIdx.x * 4 * region_words;
+        for (;;) {
+            __syncthreads();
+            if (threadIdx.x == 0)
+                team_slot = atomicAdd(counters + 32, 1);
+            __syncthreads();
+            const int64_t si = team_slot;
+            if (si >= n_team)
+                break;
+            cigar_pair<4>(q, r, p, w, pairs[si], region, slot_width, seqs,
+                          seqs + 2 * kWfaTeamSeqWords, kWfaTeamSeqWords, cost, hist_cells,
+                          arena_off, arena, runs, run_off, run_count, err_flag);
+        }
+        __syncthreads();
+    }
+    int32_t *const region = scratch + ((int64_t)blockIdx.x * 4 + wib) * region_words;
+    uint32_t *const my = seqs + wib * 4 * kWfaSeqWords;
+    for (;;) {
+        int64_t b0 = 0;
+        if (lane == 0)
+            b0 = n_team + atomicAdd(counters, 1);
+        const int64_t si = __shfl_sync(0xffffffffu, b0, 0);
+        if (si >= n)
+            break;
+        cigar_pair<1>(q, r, p, w, pairs[si], region, slot_width, my, my + 2 * kWfaSeqWords,
+                      kWfaSeqWords, cost, hist_cells, arena_off, arena, runs, run_off,
+                      run_count, err_flag);
+    }
+}
+
+cudaError_t launch_wfa_cigar(SeqView q, SeqView r, WfaParams p, const int32_t *pairs, int64_t n,
+                             int64_t n_team, int *counters, const int32_t *cost,
+                             const int64_t *hist_cells, const int64_t *arena_off, uint8_t *arena,
+                             int32_t *scratch, int64_t slot_width, int grid, uint32_t *runs,
+                             const int64_t *run_off, int32_t *run_count, int *err_flag,
+                             cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    wfa_cigar_kernel<<<grid, 128, 0, st>>>(q, r, p, pairs, n, n_team, counters, cost,
+                                           hist_cells, arena_off, arena, scratch, slot_width, runs,
+                                           run_off, run_count, err_flag);
+    return cudaGetLastError();
+}
+
+int wfa_cigar_blocks_per_sm()
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_cigar_kernel, 128, 0) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 4;
+    }
+    return nb > 0 ? nb : 1;
 }
 
 int wfa_blocks_per_sm(int variant)
