@@ -382,16 +382,20 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
                     const RT *De = se >= 0 ? D(se) : nullptr;
                     // rounds of U diagonals per thread while all U are inside
                     // [a, b], then single-diagonal rounds for the rest
-                    auto round = [&](int32_t k0, auto uc) {
+                    // FULL: every diagonal of the round lies inside [a, b] (no
+                    // liveness tests, addresses linear in u)
+                    auto round = [&](int32_t k0, auto uc, auto fc) {
                         constexpr int UU = decltype(uc)::value;
+                        constexpr bool FULL = decltype(fc)::value;
                         int32_t ks[UU], iv[UU], dv[UU], mv[UU];
                         uint32_t dec[UU];
                         bool live[UU];
 #pragma unroll
                         for (int u = 0; u < UU; ++u) {
                             ks[u] = k0 + TW * u;
-                            live[u] = ks[u] <= b;
-                            const int32_t kc = live[u] ? ks[u] : b;  // loads stay in [a-1, b+1]
+                            live[u] = FULL || ks[u] <= b;
+                            // loads stay in [a-1, b+1]
+                            const int32_t kc = FULL ? ks[u] : (live[u] ? ks[u] : b);
                             int32_t io = NEG, ie = NEG, dop = NEG, dex = NEG, mx = NEG;
                             if (Moe) {
                                 io = (int32_t)Moe[kc - 1];
@@ -445,9 +449,9 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
                     };
                     int32_t k0 = a + tt;
                     for (; k0 + TW * (U - 1) <= b; k0 += TW * U)
-                        round(k0, std::integral_constant<int, U>{});
+                        round(k0, std::integral_constant<int, U>{}, std::true_type{});
                     for (; k0 <= b; k0 += TW)
-                        round(k0, std::integral_constant<int, 1>{});
+                        round(k0, std::integral_constant<int, 1>{}, std::false_type{});
                     if (HREC)
                         hcur += wfa_hist_cell_bytes(b - a + 1) / 4;
                     // widen for the next step (see above); the positions
