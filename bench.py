@@ -560,7 +560,7 @@ def _slice(batch, i0, i1):
     return SequenceBatch.from_arrays(p[w0:w1], m[w0:w1], o[i0:i1] - w0, l[i0:i1])
 
 
-def serve_bench(dev, seconds_per_level=4.0, pool_pairs=40_000):
+def serve_bench(dev, seconds_per_level=6.0, pool_pairs=40_000):
     """Served mixed stream: Poisson arrivals of requests of 1-4,096 pairs (log-uniform),
     each pair SW (band 32/64/128) or WFA, 100-20,000 bp, divergence up to 15%.
     The peak is the completion rate with the queue kept full; each load level then

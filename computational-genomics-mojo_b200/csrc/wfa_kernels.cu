@@ -202,13 +202,14 @@ struct WfaShape {
     int g, xs, oes, es, hm, hie, nslot;
 };
 
-// Ring element: int32 (NEG = -2^30) or, when every value a pair can store
-// fits, int16 (NEG = -32768): half the ring bytes.  A value gains at most one
-// per score step, so after S = max_error/g steps rows are at most qlen + S and
-// a value that started at NEG is at most NEG + S; the caller takes int16 only
-// when qlen + S <= 32767, where NEG + S <= -1 - qlen stays negative -- so on
-// that path negative values need no renormalisation.  The int32 path stores
-// every negative result as NEG.  Arithmetic is int32 either way.
+// Ring element: int32 (NEG = -2^30) or int16 (NEG = -32768): half the ring
+// bytes.  A value gains at most one per score step, so after S steps rows are
+// at most qlen + S and a value that started at NEG is at most NEG + S.  The
+// int16 path runs only while S <= 32767 - qlen, where rows fit and
+// NEG + S <= -1 - qlen stays negative -- so negative values need no
+// renormalisation there; a pair that needs more steps returns -4 and is run
+// again with int32 rings.  The int32 path stores every negative result as
+// NEG.  Arithmetic is int32 either way.
 template <typename RT> struct RingNeg;
 template <> struct RingNeg<int32_t> {
     static constexpr int32_t value = WFA_NEG;
@@ -245,7 +246,7 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
     int64_t hbytes = 8;  // history bytes of the visited cells (score 0: one cell)
     int32_t *const hdr = reinterpret_cast<int32_t *>(hrec);
     int64_t hcur = 3 * (int64_t)hsteps;  // next free 4-byte word of the record
-    bool overrun = false;
+    bool overrun = false, need32 = false;
     if (qlen == 0 && rlen == 0) {
         result = 0;
     } else if ((int64_t)qlen + rlen + 5 > slot_width) {
@@ -298,6 +299,10 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
         } else {
             int ms = 0, is = 0;  // ring slots of the current score
             for (int64_t sp = 1; HREC ? sp < hsteps : sp * g <= max_err; ++sp) {
+                if (std::is_same<RT, int16_t>::value && sp > 32767 - (int64_t)qlen) {
+                    need32 = true;  // past the steps int16 values are proven for
+                    break;
+                }
                 const int32_t s = (int32_t)(sp * g);
                 ms = ms + 1 == hm ? 0 : ms + 1;
                 is = is + 1 == hie ? 0 : is + 1;
@@ -487,6 +492,8 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
             }
         }
     }
+    if (need32)
+        return -4;  // nothing written: the caller runs the pair with int32 rings
     if (tt == 0) {
         if (out)
             out[pi] = result;
@@ -512,22 +519,28 @@ __device__ __forceinline__ int32_t wfa_pair_dispatch(const SeqView &q, const Seq
 {
     const int64_t ql = q.lengths[pi], rl = r.lengths[pi];
     const bool smem = ((ql + 31) >> 5) < seqw && ((rl + 31) >> 5) < seqw;
-    const bool r16 = ql + p.max_error / w.g <= 32767;
-    if (smem && r16)
-        return wfa_align_pair<U, TEAM, true, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
-                                                            sq, sr, out, err_flag, work, hist,
-                                                            hrec, hlimit, hsteps);
-    if (smem)
-        return wfa_align_pair<U, TEAM, true, int32_t, HREC>(q, r, p, w, pi, region, slot_width,
-                                                            sq, sr, out, err_flag, work, hist,
-                                                            hrec, hlimit, hsteps);
+    const bool r16 = ql < 32767;
+    int32_t res = -4;
+    if (smem) {
+        if (r16)
+            res = wfa_align_pair<U, TEAM, true, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                               sq, sr, out, err_flag, work, hist,
+                                                               hrec, hlimit, hsteps);
+        if (res == -4)
+            res = wfa_align_pair<U, TEAM, true, int32_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                               sq, sr, out, err_flag, work, hist,
+                                                               hrec, hlimit, hsteps);
+        return res;
+    }
     if (r16)
-        return wfa_align_pair<U, TEAM, false, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
-                                                             sq, sr, out, err_flag, work, hist,
-                                                             hrec, hlimit, hsteps);
-    return wfa_align_pair<U, TEAM, false, int32_t, HREC>(q, r, p, w, pi, region, slot_width, sq,
-                                                         sr, out, err_flag, work, hist, hrec,
-                                                         hlimit, hsteps);
+        res = wfa_align_pair<U, TEAM, false, int16_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                            sq, sr, out, err_flag, work, hist,
+                                                            hrec, hlimit, hsteps);
+    if (res == -4)
+        res = wfa_align_pair<U, TEAM, false, int32_t, HREC>(q, r, p, w, pi, region, slot_width,
+                                                            sq, sr, out, err_flag, work, hist,
+                                                            hrec, hlimit, hsteps);
+    return res;
 }
 
 // Persistent kernel over two length-sorted queues: every block first takes

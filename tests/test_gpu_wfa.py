@@ -178,3 +178,21 @@ def test_length_classes(device, oracle):
     cfg = WFAConfig(5, 2, 3, 3000)
     ref = oracle_wfa(oracle, q, r, cfg)
     assert_same(device.wfa_affine(q, r, cfg, batched=True), ref, "(5,2,3)")
+
+
+def test_int16_step_cap_rerun(device, oracle):
+    """Queries of ~31.5 kbp whose alignments need more score steps than
+    32767 - qlen: int16 rings give up at that step and the pair is run again
+    with int32 rings; the costs equal the oracle's."""
+    rng = random.Random(31)
+    qs, rs = [], []
+    for rate in (0.03, 0.04, 0.01):
+        q = _random_seq(rng, rng.randint(31200, 31800))
+        qs.append(q)
+        rs.append(_mutate(rng, q, rate))
+    q, r = SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+    cfg = WFAConfig(4, 6, 2, 30000)
+    ref = oracle_wfa(oracle, q, r, cfg)
+    assert (ref >= 0).all() and (ref // 2 > 32767 - 31800).any()
+    for batched in (True, False):
+        assert_same(device.wfa_affine(q, r, cfg, batched=batched), ref, f"batched={batched}")

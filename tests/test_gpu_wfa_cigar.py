@@ -169,3 +169,19 @@ def test_runs_capacity_error(device):
     assert rc == GB2_ERANGE and offs[2] > 1
     q.close()
     r.close()
+
+
+def test_cigar_after_int32_rerun(device):
+    """A ~31.5 kbp pair run again with int32 rings in the CIGAR pass: its
+    CIGAR re-scores to the cost and consumes both sequences."""
+    rng = random.Random(32)
+    q = "".join(rng.choice("ACGT") for _ in range(31500))
+    r = _mutate(rng, q, 0.03)
+    cfg = WFAConfig(4, 6, 2, 30000)
+    cost, cig = device.wfa_cigar(SequenceBatch.from_strings([q]), SequenceBatch.from_strings([r]),
+                                 cfg)
+    assert cost[0] == device.wfa_affine(SequenceBatch.from_strings([q]),
+                                        SequenceBatch.from_strings([r]), cfg)[0]
+    assert cost[0] // 2 > 32767 - 31500
+    assert _cigar_cost(cig[0], 4, 6, 2) == cost[0]
+    assert _cigar_len(cig[0], "=XI") == len(q) and _cigar_len(cig[0], "=XD") == len(r)
