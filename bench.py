@@ -585,8 +585,8 @@ def serve_bench(dev, seconds_per_level=6.0, pool_pairs=40_000):
                        "or WFA (p=0.5), 100-20,000 bp log-uniform, divergence 0-15%",
            "max_error": int(wcfg.max_error)}
     with AlignmentServer(dev, hbm_budget_bytes=32 << 30, max_inflight_groups=4) as srv:
-        # peak: 64 requests submitted at once
-        reqs = [make(j) for j in range(64)]
+        # peak: 192 requests submitted at once (enough of the size mix to scale the loads)
+        reqs = [make(j) for j in range(192)]
         t0 = time.perf_counter()
         prs = [srv.submit(a, b, swc, wcfg, kinds=k, bands=bd) for a, b, bd, k in reqs]
         for pr in prs:
@@ -597,7 +597,7 @@ def serve_bench(dev, seconds_per_level=6.0, pool_pairs=40_000):
         res["peak_requests_per_s"] = round(peak, 2)
         res["peak_pairs_per_s"] = round(pairs / t_peak, 1)
         levels = []
-        jbase = 64
+        jbase = 192
         for f in (0.2, 0.4, 0.6, 0.8, 1.0):
             lam = f * peak
             n_lvl = max(8, int(lam * seconds_per_level))
