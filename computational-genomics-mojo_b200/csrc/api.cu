@@ -323,7 +323,7 @@ namespace gb2 {
 
 int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
             const gb2_sw_cfg *cfg, const int32_t *d_bands, const SwPlanInfo &pi, int64_t n,
-            gb2_sw_result *d_out, int flags)
+            gb2_sw_result *d_out, int flags, bool profile)
 {
     if (n <= 0)
         return GB2_OK;
@@ -361,7 +361,7 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
             pl.counter = (int *)x.counters.p;
             grid = c->sm_count * sw_blocks_per_sm(cls, variant);
         }
-        cudaEvent_t e0 = prof_begin(c, x.st);
+        cudaEvent_t e0 = profile ? prof_begin(c, x.st) : nullptr;
         if (cls > 0) {
             CU(c, launch_sw(cls, variant, qv, rv, p, cfg->band_width, nullptr, pl, d_out, nullptr,
                             0, grid, x.st));
@@ -427,7 +427,7 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
         return rc;
     CU(c, cudaEventRecord(x.ev_fork, x.st));
     int used = 0;
-    cudaEvent_t e0 = prof_begin(c, x.st);
+    cudaEvent_t e0 = profile ? prof_begin(c, x.st) : nullptr;
     for (int k = 0; k < kSwClasses; ++k) {
         if (!need[k])
             continue;
@@ -1023,6 +1023,8 @@ int gb2_create(int device, gb2_ctx **out)
         if (ok)
             cudaEventRecord(c->pin_ev[i], c->x.st);
     }
+    for (int i = 0; ok && i < kResidentParts; ++i)
+        ok = cudaEventCreateWithFlags(&c->kdone[i], cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < kPipeSets; ++i) {
         ok = cudaEventCreateWithFlags(&c->pipe[i].copied, cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pipe[i].done, cudaEventDisableTiming) == cudaSuccess;
@@ -1074,6 +1076,9 @@ int gb2_destroy(gb2_ctx *c)
         if (ps.done)
             cudaEventDestroy(ps.done);
     }
+    for (int i = 0; i < kResidentParts; ++i)
+        if (c->kdone[i])
+            cudaEventDestroy(c->kdone[i]);
     for (int i = 0; i < 2; ++i) {
         if (c->pin[i])
             cudaFreeHost(c->pin[i]);
@@ -1236,10 +1241,61 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
             return rc;
         d_bands = (const int32_t *)c->bands.p;
     }
-    if ((rc = sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands, pi, n,
-                      (gb2_sw_result *)c->out_sw.p, flags)))
+    // Large batches run as kResidentParts parts alternating between the two
+    // executors, each part's results copied back while the next part computes.
+    const int parts = n >= kResidentSplit ? kResidentParts : 1;
+    if (parts == 1) {
+        if ((rc = sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands,
+                          pi, n, (gb2_sw_result *)c->out_sw.p, flags)))
+            return rc;
+        return d2h_results(c, out, c->out_sw.p, (size_t)n * sizeof(gb2_sw_result));
+    }
+    const bool out_pinned = is_pinned(out);
+    if (!out_pinned && (rc = pin_out(c, (size_t)n * sizeof(gb2_sw_result))))
         return rc;
-    return d2h_results(c, out, c->out_sw.p, (size_t)n * sizeof(gb2_sw_result));
+    gb2_sw_result *const host = out_pinned ? out : (gb2_sw_result *)c->pin_out;
+    gb2_sw_result *const dres = (gb2_sw_result *)c->out_sw.p;
+    CU(c, cudaEventRecord(c->x.ev_fork, c->x.st));  // bands copied before either executor runs
+    CU(c, cudaStreamWaitEvent(c->x2.st, c->x.ev_fork, 0));
+    // profiling: one span per call, from the first part's start to the later of
+    // the two executors' last kernels (the parts overlap, so their own
+    // durations would double-count)
+    cudaEvent_t span0 = prof_begin(c, c->x.st);
+    const int64_t per = (n + parts - 1) / parts;
+    for (int k = 0; k < parts && rc == GB2_OK; ++k) {
+        const int64_t p0 = k * per, m = std::min(per, n - p0);
+        Exec &ex = (k & 1) ? c->x2 : c->x;
+        SeqView qv = view_of(q), rv = view_of(r);
+        qv.offsets += p0;
+        qv.lengths += p0;
+        rv.offsets += p0;
+        rv.lengths += p0;
+        rc = sw_core(c, ex, qv, rv, q->max_len, r->max_len, cfg, d_bands ? d_bands + p0 : nullptr,
+                     pi, m, dres + p0, flags, false);
+        if (!rc && cudaEventRecord(c->kdone[k], ex.st) != cudaSuccess)
+            rc = set_err(c, GB2_ECUDA, "event record failed");
+        if (!rc && cudaMemcpyAsync(host + p0, dres + p0, (size_t)m * sizeof(gb2_sw_result),
+                                   cudaMemcpyDeviceToHost, ex.st) != cudaSuccess)
+            rc = set_err(c, GB2_ECUDA, "result copy failed");
+    }
+    if (span0 && !rc) {
+        cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 2], 0);
+        cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 1], 0);
+        prof_end(c, span0, c->st_copy);
+    } else if (span0) {
+        cudaEventDestroy(span0);
+    }
+    const cudaError_t e2 = cudaStreamSynchronize(c->x2.st);
+    const int rc2 = sync_and_check(c);
+    if (rc)
+        return rc;
+    if (e2 != cudaSuccess)
+        return set_err(c, GB2_ECUDA, "second executor: %s", cudaGetErrorString(e2));
+    if (rc2)
+        return rc2;
+    if (!out_pinned)
+        memcpy(out, c->pin_out, (size_t)n * sizeof(gb2_sw_result));
+    return GB2_OK;
 }
 
 int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,

@@ -49,6 +49,8 @@ struct PipeSet {
     cudaEvent_t copied = nullptr, done = nullptr;
 };
 constexpr int kPipeSets = 3;  // chunks in flight in the host pipeline
+constexpr int64_t kResidentSplit = 1 << 18;  // resident SW batches this large run in parts
+constexpr int kResidentParts = 4;
 
 struct SwPlanInfo {
     bool fast_ok;       // the register kernels apply (sign conditions on the scores)
@@ -96,6 +98,7 @@ struct gb2_ctx {
     size_t pin_out_cap = 0;
     gb2::PipeSet pipe[gb2::kPipeSets];
     gb2::CigarBufs cig;
+    cudaEvent_t kdone[gb2::kResidentParts] = {};  // last kernel of each resident part
     // statistics
     std::atomic<bool> profiling{false};
     std::mutex prof_mu;
@@ -133,9 +136,10 @@ void harvest_profile(gb2_ctx *c);
 int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n, int64_t qmax,
                 int64_t rmax, SwPlanInfo &pi);
 // Enqueues Smith-Waterman for n pairs of (qv, rv) on executor x; results to d_out.
+// profile: record the launches' duration when the context is profiling.
 int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
             const gb2_sw_cfg *cfg, const int32_t *d_bands, const SwPlanInfo &pi, int64_t n,
-            gb2_sw_result *d_out, int flags);
+            gb2_sw_result *d_out, int flags, bool profile = true);
 int wfa_validate(gb2_ctx *c, const gb2_wfa_cfg *cfg, int64_t n);
 // Clears the WFA error flag and work counter of x (once per call, before the
 // first wfa_core of that call).
