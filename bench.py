@@ -338,7 +338,8 @@ def our_arm(args, dist: Dist):
         packed = BAND <= 32 and SCORING[0] * 150 <= 511
         ops_per_cell = SW_OPS_PER_CELL_PACKED if packed else SW_OPS_PER_CELL
         achieved_ops = kern_gcups * ops_per_cell
-        alg_bytes = h2d - 0 + d2h  # packed words + metadata read, results written
+        # the kernel reads the packed words and int64 offsets and lengths, writes results
+        alg_bytes = q.packed.nbytes + r.packed.nbytes + 32 * args.pairs + d2h
         mp = {}
         mp_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
         if os.path.exists(mp_path):
