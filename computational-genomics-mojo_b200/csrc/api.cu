@@ -703,29 +703,24 @@ static void scan_side(const HostSide &h, int64_t i0, int64_t i1, int64_t &w0, in
     contig = ct;
 }
 
-static ChunkScan scan_chunk(const HostSide &hq, const HostSide &hr, int64_t p0, int64_t p1,
-                            int32_t *q32, int32_t *r32)
+// One side's part of a chunk scan.
+struct SideScan {
+    int64_t w0 = 0, w1 = 0, minlen = 0, maxlen = 0, bits = 0;
+    bool contig = true;
+};
+
+static ChunkScan combine(const SideScan &q, const SideScan &r)
 {
-    int64_t qlo, qhi, qmn, qmx, qb, rlo, rhi, rmn, rmx, rb;
-    bool qc, rc;
-    if (p1 - p0 >= (1 << 16)) {
-        std::thread t([&] { scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb, rc, r32); });
-        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb, qc, q32);
-        t.join();
-    } else {
-        scan_side(hq, p0, p1, qlo, qhi, qmn, qmx, qb, qc, q32);
-        scan_side(hr, p0, p1, rlo, rhi, rmn, rmx, rb, rc, r32);
-    }
     ChunkScan o;
-    o.negative = (qb | rb) < 0;
-    o.qw0 = qlo;
-    o.qw1 = std::max(qhi, qlo);
-    o.rw0 = rlo;
-    o.rw1 = std::max(rhi, rlo);
-    o.qmaxlen = qmx;
-    o.rmaxlen = rmx;
-    o.narrow = narrow_range(qmn, qmx) && narrow_range(rmn, rmx);
-    o.dense = qc && rc && qmx < (1ll << 31) && rmx < (1ll << 31);
+    o.negative = (q.bits | r.bits) < 0;
+    o.qw0 = q.w0;
+    o.qw1 = std::max(q.w1, q.w0);
+    o.rw0 = r.w0;
+    o.rw1 = std::max(r.w1, r.w0);
+    o.qmaxlen = q.maxlen;
+    o.rmaxlen = r.maxlen;
+    o.narrow = narrow_range(q.minlen, q.maxlen) && narrow_range(r.minlen, r.maxlen);
+    o.dense = q.contig && r.contig && q.maxlen < (1ll << 31) && r.maxlen < (1ll << 31);
     return o;
 }
 
@@ -841,18 +836,18 @@ k_expand_write(int64_t m, const int32_t *__restrict__ q32, const int32_t *__rest
     }
 }
 
-// Grows a pipe set's pinned int32 staging (its previous copy has completed).
-static int ensure_len32(gb2_ctx *c, PipeSet &ps, size_t bytes)
+// Grows the context's pinned int32 length staging of the host pipeline.
+static int ensure_len32(gb2_ctx *c, size_t bytes)
 {
-    if (bytes <= ps.h_len32_cap)
+    if (bytes <= c->pin_len32_cap)
         return GB2_OK;
-    if (ps.h_len32)
-        cudaFreeHost(ps.h_len32);
-    ps.h_len32 = nullptr;
-    ps.h_len32_cap = 0;
+    if (c->pin_len32)
+        cudaFreeHost(c->pin_len32);
+    c->pin_len32 = nullptr;
+    c->pin_len32_cap = 0;
     const size_t cap = std::max<size_t>(bytes + bytes / 4, 1 << 16);
-    CU(c, cudaMallocHost(&ps.h_len32, cap));
-    ps.h_len32_cap = cap;
+    CU(c, cudaMallocHost(&c->pin_len32, cap));
+    c->pin_len32_cap = cap;
     return GB2_OK;
 }
 
@@ -864,32 +859,63 @@ static int ensure_len32(gb2_ctx *c, PipeSet &ps, size_t bytes)
 // one of the context's two executors (alternating, so one chunk's kernels can
 // fill the GPU while the previous chunk's last blocks drain); results come
 // back on the executor's stream.  kPipeSets chunks are in flight: the copies
-// of a chunk wait on the device for the chunk that last used its buffers,
-// and the host waits only before reusing pinned staging that may still be
-// read.  On any error every stream is drained before returning, so no copy
+// of a chunk wait on the device for the chunk that last used its buffers.  On any error every stream is drained before returning, so no copy
 // touches the caller's memory after the call.
 template <typename RunChunk>
 static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const int32_t *bands,
                     int64_t n, size_t out_elem, void *out_host, int64_t chunk_pairs,
                     RunChunk run_chunk)
 {
-    const int64_t nchunks = (n + chunk_pairs - 1) / chunk_pairs;
+    std::vector<int64_t> bounds{0};
+    while (bounds.back() < n)
+        bounds.push_back(std::min(n, bounds.back() + chunk_pairs));
+    const int64_t nchunks = (int64_t)bounds.size() - 1;
     int rc = GB2_OK;
     const bool out_pinned = is_pinned(out_host);
     if (!out_pinned && (rc = pin_out(c, (size_t)n * out_elem)))
         return rc;
+    // Two scanner threads (one per side) run through all chunks ahead of the
+    // issuing thread, writing each chunk's int32 lengths into pinned staging
+    // (chunk [p0, p1): q at 2*p0, r right after) and publishing the chunk's
+    // scan; the issuing thread waits only for chunks not scanned yet.  The
+    // staging is the context's and is free: the previous call's copies ended
+    // before it returned.
+    if ((rc = ensure_len32(c, (size_t)n * 8)))
+        return rc;
+    int32_t *const stage = (int32_t *)c->pin_len32;
+    std::vector<SideScan> sq((size_t)nchunks), sr((size_t)nchunks);
+    std::atomic<int64_t> q_done{0}, r_done{0};
+    auto scanner = [&](const HostSide &h, std::vector<SideScan> *out, std::atomic<int64_t> *done,
+                       int side) {
+        for (int64_t ci = 0; ci < nchunks; ++ci) {
+            const int64_t p0 = bounds[(size_t)ci], p1 = bounds[(size_t)ci + 1];
+            SideScan &sc = (*out)[(size_t)ci];
+            scan_side(h, p0, p1, sc.w0, sc.w1, sc.minlen, sc.maxlen, sc.bits, sc.contig,
+                      stage + 2 * p0 + (side ? p1 - p0 : 0));
+            done->store(ci + 1, std::memory_order_release);
+        }
+    };
+    std::thread tq(scanner, std::cref(hq), &sq, &q_done, 0);
+    std::thread tr(scanner, std::cref(hr), &sr, &r_done, 1);
+    struct Joiner {
+        std::thread &a, &b;
+        ~Joiner()
+        {
+            a.join();
+            b.join();
+        }
+    } joiner{tq, tr};
     auto issue = [&](int64_t ci) -> int {
         PipeSet &ps = c->pipe[ci % kPipeSets];
         Exec &x = (ci & 1) ? c->x2 : c->x;
-        const int64_t p0 = ci * chunk_pairs, p1 = std::min(n, p0 + chunk_pairs);
+        const int64_t p0 = bounds[(size_t)ci], p1 = bounds[(size_t)ci + 1];
         const int64_t m = p1 - p0;
         int r;
-        // the staging of this set's previous chunk has been copied
-        CU(c, cudaEventSynchronize(ps.copied));
-        if ((r = ensure_len32(c, ps, (size_t)m * 8)))
-            return r;
-        int32_t *q32 = (int32_t *)ps.h_len32, *r32 = q32 + m;
-        const ChunkScan cs = scan_chunk(hq, hr, p0, p1, q32, r32);
+        while (q_done.load(std::memory_order_acquire) <= ci ||
+               r_done.load(std::memory_order_acquire) <= ci)
+            std::this_thread::yield();
+        int32_t *q32 = stage + 2 * p0;
+        const ChunkScan cs = combine(sq[(size_t)ci], sr[(size_t)ci]);
         if (cs.negative)
             return set_err(c, GB2_EINVAL, "negative offset or length among pairs %lld-%lld",
                            (long long)p0, (long long)(p1 - 1));
@@ -1069,8 +1095,6 @@ int gb2_destroy(gb2_ctx *c)
         for (DevBuf *b : pb)
             if (b->p)
                 cudaFree(b->p);
-        if (ps.h_len32)
-            cudaFreeHost(ps.h_len32);
         if (ps.copied)
             cudaEventDestroy(ps.copied);
         if (ps.done)
@@ -1087,6 +1111,8 @@ int gb2_destroy(gb2_ctx *c)
     }
     if (c->pin_out)
         cudaFreeHost(c->pin_out);
+    if (c->pin_len32)
+        cudaFreeHost(c->pin_len32);
     if (c->t0)
         cudaEventDestroy(c->t0);
     if (c->t1)

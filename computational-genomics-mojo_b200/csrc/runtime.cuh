@@ -44,8 +44,6 @@ constexpr int64_t kCigarArenaCap = 16ll << 30;  // WFA history arena, bytes at m
 // One set of device buffers of the end-to-end pipeline.
 struct PipeSet {
     DevBuf qw, rw, qo, ql, ro, rl, bands, out, len32;
-    void *h_len32 = nullptr;  // pinned int32 lengths of a contiguous chunk (q then r)
-    size_t h_len32_cap = 0;
     cudaEvent_t copied = nullptr, done = nullptr;
 };
 constexpr int kPipeSets = 3;  // chunks in flight in the host pipeline
@@ -96,6 +94,8 @@ struct gb2_ctx {
     std::mutex pin_mu;
     void *pin_out = nullptr;
     size_t pin_out_cap = 0;
+    void *pin_len32 = nullptr;  // int32 lengths of contiguous chunks (host pipeline)
+    size_t pin_len32_cap = 0;
     gb2::PipeSet pipe[gb2::kPipeSets];
     gb2::CigarBufs cig;
     cudaEvent_t kdone[gb2::kResidentParts] = {};  // last kernel of each resident part
