@@ -480,7 +480,8 @@ int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t
     pi.fast_ok = cfg->gap_extend <= 0 && cfg->gap_open + cfg->gap_extend <= 0 && cfg->mismatch <= 0;
     const int32_t goe = cfg->gap_open + cfg->gap_extend;
     pi.pack_ok = pi.fast_ok && cfg->mismatch >= goe && cfg->match_score >= cfg->mismatch &&
-                 cfg->match_score <= 255 && -goe <= 255 && -cfg->gap_extend <= 255;
+                 cfg->match_score <= 255 && -goe <= 255 && -cfg->gap_extend <= 255 &&
+                 cfg->match_score - cfg->mismatch <= 255;
     pi.max_band = maxb;
     pi.uniform_band = bands == nullptr;
     return GB2_OK;

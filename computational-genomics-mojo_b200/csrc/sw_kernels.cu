@@ -261,20 +261,73 @@ sw_band_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__r
 // Bits: H <= 511 in every cell (the host checks match*min(qlen, rlen)), all
 // terms stay inside int16, the first-maximum key H*128 + (127-column) fits
 // an unsigned 16-bit half, and the per-half subtract of |go+ge| cannot
-// borrow because H' >= |go+ge|.  The substitution score comes from the
-// equality bits of both rows: s = eqL | eqH << 16, sub - (go+ge) =
-// s*(match-mismatch) + (mismatch-(go+ge)) with mismatch >= go+ge, so the
-// multiply-add never carries between halves.
+// borrow because H' >= |go+ge|.
+//
+// Pipe balance.  The three DPX max instructions per register run on the
+// integer ALU pipe, which this recurrence saturates; the FMA pipe (integer
+// multiply-add) is a separate pipe of the same width.  So every step that a
+// multiply-add can do runs there, with multipliers passed as kernel
+// arguments (Pack16Consts) so the compiler cannot turn them back into
+// shifts:
+//  - the substitution score of both cells of a register is one mad.hi: the
+//    equality bits of the two cells sit at bits p and p+16 of a word, and
+//    hi32(bits * ((match-mismatch) << (32-p))) + (mismatch-(go+ge)) in both
+//    halves is exact while (match-mismatch) << (32-p) fits 32 bits (p >= 8
+//    here; the host requires match-mismatch <= 255);
+//  - the -(go+ge) subtract, the key H*128 + tag, the two-bit shifts that
+//    slide the reference window and the previous row's equality bits, and
+//    the one-bit shift of the equality test are multiply-adds or mad.hi.
+// Sequences are read as 16-base (32-bit) words, reloaded every 16 rows; the
+// reference word entering the window and the query word are consumed two
+// bits per row by multiplication.
 // ---------------------------------------------------------------------------
-// One step of sw_pack16_kernel over all R registers.  MASK = false when every
-// cell of the step lies inside the matrix (the common case); MASK = true
-// zeroes the first-maximum keys of cells past the query or reference end.
-// Returns the packed row keys: low half row t, high half row t-1.
+// Constants of sw_pack16_kernel, built by the host from SwParams.  The
+// multipliers (1, 4, 128, 256, 2^31 and the shifted score difference) are
+// kernel arguments rather than literals so that the multiply-adds using them
+// stay multiply-adds.
+struct Pack16Consts {
+    uint32_t one, x4, x128, x256, half;
+    uint32_t dm[4];  // (match - mismatch) << 18, 20, 22, 24
+    uint32_t mmg2;   // mismatch - (go+ge) in both halves
+    uint32_t neg_g2; // minus -(go+ge) in both halves, mod 2^32
+    uint32_t ge2;    // ge in both halves
+    uint32_t ng2;    // -(go+ge) in both halves
+};
+
+__device__ __forceinline__ uint32_t mad_hi_u32(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// (a << 2) | (b >> 30) as two multiply-adds (x4 == 4).
+__device__ __forceinline__ uint32_t shl2_in(uint32_t a, uint32_t b, uint32_t x4)
+{
+    return a * x4 + mad_hi_u32(b, x4, 0u);
+}
+
+// 16-base word k (bases 16k..16k+15, first base in the top two bits) of the
+// 2-bit MSB-first sequence starting at 64-bit word `off`; k is clamped into
+// the packed array (the clamped words are never read by an in-matrix cell).
+__device__ __forceinline__ uint32_t seq_word16(const SeqView &s, int64_t off, int64_t k)
+{
+    int64_t i = 2 * off + (k ^ 1);
+    const int64_t last = 2 * s.n_words - 1;
+    i = i < 0 ? 0 : (i > last ? last : i);
+    return __ldg(reinterpret_cast<const uint32_t *>(s.packed) + i);
+}
+
+// One step of sw_pack16_kernel over all R registers.  eq[k] / bw[k]: the
+// equality bits (bit 30-2c for column 16k+c) of row t and of row t-1 shifted
+// so column B+1+h sits where column h does.  MASK = false when every cell of
+// the step lies inside the matrix (the common case); MASK = true zeroes the
+// first-maximum keys of cells past the query or reference end.  Returns the
+// packed row keys: low half row t, high half row t-1.
 template <int B, bool MASK>
-__device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const uint64_t *eqc,
-                                                 const uint64_t *bw, uint32_t &e_last, int limL,
-                                                 int limH, uint32_t GE2, uint32_t NG2,
-                                                 uint32_t GOE_SUB, uint32_t MMG2, uint32_t DM)
+__device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const uint32_t *eq,
+                                                 const uint32_t *bw, uint32_t &e_last, int limL,
+                                                 int limH, const Pack16Consts &c)
 {
     constexpr int NL = B + 1, R = NL;
     const uint32_t SENT = 0x0000C000u;
@@ -284,16 +337,18 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
     uint32_t rk = 0, kpend = 0;
 #pragma unroll
     for (int h = 0; h < R; ++h) {
-        const int k = h >> 4, j = h & 15;
-        const uint32_t a32 = (k & 1) ? (uint32_t)eqc[k >> 1] : (uint32_t)(eqc[k >> 1] >> 32);
-        const uint32_t b32 = (k & 1) ? (uint32_t)bw[k >> 1] : (uint32_t)(bw[k >> 1] >> 32);
-        const uint32_t wsel = (j < 8) ? __byte_perm(a32, b32, 0x7632) : __byte_perm(a32, b32, 0x5410);
-        const int pos = (j < 8) ? (14 - 2 * j) : (30 - 2 * j);
-        const uint32_t sub = ((wsel >> pos) & 0x00010001u) * DM + MMG2;
+        const int k = h >> 4, j = h & 15, jj = h & 7;
+        // cells 8*(h>>3) .. +7 of both halves at bits 14-2*jj and 30-2*jj
+        const uint32_t wsel = (j < 8) ? __byte_perm(eq[k], bw[k], 0x7632)
+                                      : __byte_perm(eq[k], bw[k], 0x5410);
+        const uint32_t wv = (jj < 4) ? wsel : wsel * c.x256;  // cells 4..7 up to bits 14..8
+        const int pos = 14 - 2 * (jj & 3);
+        const uint32_t sub =
+            mad_hi_u32(wv & ((1u << pos) | (1u << (pos + 16))), c.dm[jj & 3], c.mmg2);
         const uint32_t up = (h + 1 < R) ? Hr[h + 1 < R ? h + 1 : h] : (h0new >> 16);
-        const uint32_t e = __viaddmax_s16x2(el, GE2, up);
-        const uint32_t tt = __vimax3_s16x2(e, hl, NG2);
-        uint32_t hn = __viaddmax_s16x2(Hr[h], sub, tt) - GOE_SUB;
+        const uint32_t e = __viaddmax_s16x2(el, c.ge2, up);
+        const uint32_t tt = __vimax3_s16x2(e, hl, c.ng2);
+        uint32_t hn = __viaddmax_s16x2(Hr[h], sub, tt) * c.one + c.neg_g2;
         if (h == R - 1)
             hn &= 0x0000FFFFu;  // padding column stays 0
         if (h == 0)
@@ -301,7 +356,7 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
         Hr[h] = hn;
         hl = hn;
         el = e;
-        uint32_t key = hn * 128u + (((uint32_t)(127 - h)) | ((uint32_t)(127 - NL - h) << 16));
+        uint32_t key = hn * c.x128 + (((uint32_t)(127 - h)) | ((uint32_t)(127 - NL - h) << 16));
         if (MASK)
             key &= (h < limL ? 0x0000FFFFu : 0u) | (h < limH ? 0xFFFF0000u : 0u);
         if (h & 1)
@@ -317,15 +372,18 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
 
 template <int B>
 __global__ void __launch_bounds__(128)
-sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__restrict__ out)
+sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_result *__restrict__ out)
 {
+    static_assert(B % 16 == 0, "band must be a multiple of 16");
     constexpr int W = 2 * B + 1;
     constexpr int NL = B + 1;           // columns in low halves
     constexpr int R = NL;               // registers
-    constexpr int NWIN = (W + 31) / 32; // 64-bit eq words of one row
-    constexpr int SHIFT = 2 * NL;       // bits between column h and column NL+h
-    constexpr int SW_ = SHIFT / 64, SB_ = SHIFT % 64;
+    constexpr int NE = (W + 15) / 16;   // 16-column equality words of one row
+    constexpr int BW0 = NL / 16;        // first word of columns B+1.. (offset one column)
+    constexpr int NBW = B / 16;         // shifted words of the previous row
+    constexpr int RW0 = NE - B / 16;    // 16-base word entering the window at t = 0
     static_assert(W <= 127, "column index must fit the key");
+    static_assert(NL % 16 == 1 && BW0 + NBW < NE, "word layout");
 
     int64_t n;
     const int32_t *__restrict__ queue = pairs_resolve(pl, n);
@@ -334,13 +392,6 @@ sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *_
     const int warps_per_block = blockDim.x >> 5;
     const int64_t warp_global = (int64_t)blockIdx.x * warps_per_block + (threadIdx.x >> 5);
     const int64_t warps_total = (int64_t)gridDim.x * warps_per_block;
-
-    const int32_t goe = p.go + p.ge;  // <= 0
-    const uint32_t GE2 = ((uint32_t)(uint16_t)p.ge) * 0x00010001u;
-    const uint32_t NG2 = ((uint32_t)(uint16_t)(-goe)) * 0x00010001u;
-    const uint32_t GOE_SUB = (uint32_t)(-goe) * 0x00010001u;
-    const uint32_t MMG2 = (uint32_t)(p.mismatch - goe) * 0x00010001u;
-    const uint32_t DM = (uint32_t)(p.match - p.mismatch);
     const uint32_t SENT = 0x0000C000u;  // -16384 in the low half
 
     int64_t base = warp_global * 32;
@@ -363,91 +414,66 @@ sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *_
 #pragma unroll
             for (int h = 0; h < R; ++h)
                 Hr[h] = 0;
-            uint64_t eqp[NWIN + 1];
+            uint32_t ep[NE];  // equality bits of the previous row
 #pragma unroll
-            for (int i = 0; i <= NWIN; ++i)
-                eqp[i] = 0;
+            for (int i = 0; i < NE; ++i)
+                ep[i] = 0;
+            // The reference window of row t, r[t-B .. t-B+16*NE), one 16-base word
+            // per entry, slid by one base per row; the base entering at the bottom
+            // is the top of `rw`, the word of positions t-B+16*NE.., reloaded every
+            // 16 rows (t-B+16*NE is a multiple of 16 exactly when t is).  Words
+            // before the reference start are zero and masked below.
+            uint32_t win[NE];
+#pragma unroll
+            for (int i = 0; i < NE; ++i)
+                win[i] = (i < B / 16) ? 0u : seq_word16(r, roff, i - B / 16);
             uint32_t e_last = SENT;
-            uint32_t saved_lowkey = 0;
-            int32_t best = 0, bq = 0, bc = 0;
+            uint32_t saved_lowkey = 0, bestkey = 0, thr = 127;
+            int32_t bq = 0;
+            uint32_t qw = 0, rw = 0;
+            uint32_t qn = seq_word16(q, qoff, 0), rn = seq_word16(r, roff, RW0);  // next words
             const int steps = qlen > 0 ? qlen + 1 : 0;
-            // The reference window of row t, r[t-B .. t-B+32*NWIN), as 2-bit codes in
-            // NWIN words: built once here, then slid by one base per row; the base
-            // entering at the bottom comes from `rnext`, the reference word holding
-            // position t-B+32*NWIN, reloaded every 32 rows.  Bases before the
-            // reference start are masked below, bases past its end are never read
-            // by an in-matrix cell; loads are clamped to the packed array.
-            uint64_t win[NWIN];
-            {
-                const int64_t w = roff + ((int64_t)(-B) >> 5);
-                const int sh = (int)((-B) & 31) * 2;
-                uint64_t words[NWIN + 1];
-#pragma unroll
-                for (int i = 0; i <= NWIN; ++i) {
-                    int64_t wi = w + i;
-                    wi = wi < 0 ? 0 : (wi >= r.n_words ? r.n_words - 1 : wi);
-                    words[i] = __ldg(r.packed + wi);
-                }
-#pragma unroll
-                for (int i = 0; i < NWIN; ++i)
-                    win[i] = sh ? ((words[i] << sh) | (words[i + 1] >> (64 - sh))) : words[i];
-            }
-            const int64_t rbase = roff + ((int64_t)(32 * NWIN - B) >> 5);  // word of pos 32*NWIN-B
-            int rsub = (32 * NWIN - B) & 31;  // position of the entering base within rnext
-            int64_t rwi = rbase < r.n_words ? rbase : r.n_words - 1;
-            uint64_t rnext = __ldg(r.packed + rwi);
-            uint64_t qword = 0;
+            const int full_end = min(qlen, rlen - B + 1);  // rows t < full_end lie inside
             for (int t = 0; t < steps; ++t) {
+                if ((t & 15) == 0) {  // words of rows t..t+15; fetch the following ones
+                    qw = qn;
+                    rw = rn;
+                    qn = seq_word16(q, qoff, (t >> 4) + 1);
+                    rn = seq_word16(r, roff, (t >> 4) + RW0 + 1);
+                }
                 // equality bits of row t against its window r[t-B .. t+B]
-                uint64_t eqc[NWIN + 1];
-                eqc[NWIN] = 0;
-                if (t < qlen) {
-                    if ((t & 31) == 0)
-                        qword = __ldg(q.packed + qoff + (t >> 5));
-                    const uint64_t qrep = ((qword >> (62 - 2 * (t & 31))) & 3u) * 0x5555555555555555ull;
-                    const int64_t ri0 = (int64_t)t - B;
+                const uint32_t qrep = mad_hi_u32(qw, c.x4, 0u) * 0x55555555u;
+                qw *= c.x4;
+                uint32_t eq[NE];
 #pragma unroll
-                    for (int i = 0; i < NWIN; ++i) {
-                        const uint64_t x = win[i] ^ qrep;
-                        eqc[i] = ~(x | (x >> 1)) & 0x5555555555555555ull;
-                    }
-                    // slide the window one base for row t+1
-                    const uint64_t enter = (rnext >> (62 - 2 * rsub)) & 3u;
-#pragma unroll
-                    for (int i = 0; i + 1 < NWIN; ++i)
-                        win[i] = (win[i] << 2) | (win[i + 1] >> 62);
-                    win[NWIN - 1] = (win[NWIN - 1] << 2) | enter;
-                    if (++rsub == 32) {
-                        rsub = 0;
-                        ++rwi;
-                        rnext = __ldg(r.packed + (rwi < r.n_words ? rwi : r.n_words - 1));
-                    }
-                    if (ri0 < 0) {  // columns before the reference start never match
-                        const int64_t nneg = -ri0;
-#pragma unroll
-                        for (int i = 0; i < NWIN; ++i) {
-                            const int64_t cnt = nneg - 32 * i;
-                            if (cnt >= 32)
-                                eqc[i] = 0;
-                            else if (cnt > 0)
-                                eqc[i] &= (~0ull) >> (2 * cnt);
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < NWIN; ++i)
-                        eqc[i] = 0;
+                for (int i = 0; i < NE; ++i) {
+                    const uint32_t x = win[i] ^ qrep;
+                    eq[i] = ~(x | mad_hi_u32(x, c.half, 0u)) & 0x55555555u;
                 }
-                // previous row's bits, shifted so column NL+h sits where column h does
-                uint64_t bw[NWIN];
+                if (t < B) {  // columns before the reference start never match
 #pragma unroll
-                for (int i = 0; i < NWIN; ++i) {
-                    const uint64_t a = (i + SW_ <= NWIN) ? eqp[i + SW_] : 0;
-                    const uint64_t b = (i + SW_ + 1 <= NWIN) ? eqp[i + SW_ + 1] : 0;
-                    bw[i] = SB_ ? ((a << SB_) | (b >> (64 - SB_))) : a;
+                    for (int i = 0; i < NE; ++i) {
+                        const int cnt = B - t - 16 * i;
+                        if (cnt >= 16)
+                            eq[i] = 0;
+                        else if (cnt > 0)
+                            eq[i] &= 0xFFFFFFFFu >> (2 * cnt);
+                    }
                 }
-                // does any cell of this step fall outside the matrix?
-                const bool full = (t >= 1) && (t < qlen) && (t + B - 1 < rlen);
+                // slide the window one base for row t+1
+#pragma unroll
+                for (int i = 0; i + 1 < NE; ++i)
+                    win[i] = shl2_in(win[i], win[i + 1], c.x4);
+                win[NE - 1] = shl2_in(win[NE - 1], rw, c.x4);
+                rw *= c.x4;
+                // previous row's bits, shifted so column NL+h sits where column h does;
+                // the last word holds only the padding column
+                uint32_t bw[NBW + 1];
+#pragma unroll
+                for (int i = 0; i < NBW; ++i)
+                    bw[i] = shl2_in(ep[BW0 + i], ep[BW0 + i + 1], c.x4);
+                bw[NBW] = 0;
+                const bool full = t >= 1 && t < full_end;
                 int limL = 0, limH = 0;
                 if (!full) {
                     if (t < qlen)
@@ -455,24 +481,23 @@ sw_pack16_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *_
                     if (t >= 1 && t - 1 < qlen)
                         limH = max(0, min(R, rlen - (t - 1 - B + NL)));
                 }
-                const uint32_t rk =
-                    full ? pack16_cells<B, false>(Hr, eqc, bw, e_last, 0, 0, GE2, NG2, GOE_SUB,
-                                                  MMG2, DM)
-                         : pack16_cells<B, true>(Hr, eqc, bw, e_last, limL, limH, GE2, NG2,
-                                                 GOE_SUB, MMG2, DM);
-                // row t-1 is complete: its first half came one step earlier
-                const uint32_t highkey = rk >> 16, lowkey = rk & 0xFFFFu;
-                const uint32_t rowkey = max(saved_lowkey, highkey);
-                if ((int32_t)(rowkey >> 7) > best) {
-                    best = (int32_t)(rowkey >> 7);
+                const uint32_t rk = full ? pack16_cells<B, false>(Hr, eq, bw, e_last, 0, 0, c)
+                                         : pack16_cells<B, true>(Hr, eq, bw, e_last, limL, limH, c);
+                // row t-1 is complete: its first half came one step earlier; a key
+                // above thr = bestkey | 127 has a larger H than the best so far
+                const uint32_t rowkey = max(saved_lowkey, rk >> 16);
+                if (rowkey > thr) {
+                    thr = rowkey | 127u;
+                    bestkey = rowkey;
                     bq = t - 1;
-                    bc = 127 - (int32_t)(rowkey & 127u);
                 }
-                saved_lowkey = lowkey;
+                saved_lowkey = rk & 0xFFFFu;
 #pragma unroll
-                for (int i = 0; i < NWIN; ++i)
-                    eqp[i] = eqc[i];
+                for (int i = 0; i < NE; ++i)
+                    ep[i] = eq[i];
             }
+            const int32_t best = (int32_t)(bestkey >> 7);
+            const int32_t bc = 127 - (int32_t)(bestkey & 127u);
             gb2_sw_result res;
             res.score = best;
             res.query_end = best > 0 ? bq : 0;
@@ -629,10 +654,23 @@ cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParam
                 return pl.n <= 0 && !pl.seg ? cudaSuccess : cudaErrorInvalidValue;
             g = (int)((pl.n + 127) / 128);
         }
+        const uint32_t gg = (uint32_t)(-(p.go + p.ge)), dm = (uint32_t)(p.match - p.mismatch);
+        Pack16Consts c;
+        c.one = 1;
+        c.x4 = 4;
+        c.x128 = 128;
+        c.x256 = 256;
+        c.half = 0x80000000u;
+        for (int i = 0; i < 4; ++i)
+            c.dm[i] = dm << (18 + 2 * i);
+        c.mmg2 = ((uint32_t)p.mismatch + gg) * 0x00010001u;
+        c.neg_g2 = 0u - gg * 0x00010001u;
+        c.ge2 = (uint32_t)(uint16_t)p.ge * 0x00010001u;
+        c.ng2 = (uint32_t)(uint16_t)gg * 0x00010001u;
         if (band_class == (16 | kPack16))
-            sw_pack16_kernel<16><<<g, 128, 0, st>>>(q, r, p, pl, out);
+            sw_pack16_kernel<16><<<g, 128, 0, st>>>(q, r, c, pl, out);
         else
-            sw_pack16_kernel<32><<<g, 128, 0, st>>>(q, r, p, pl, out);
+            sw_pack16_kernel<32><<<g, 128, 0, st>>>(q, r, c, pl, out);
         return cudaGetLastError();
     }
     case 16:

@@ -548,9 +548,10 @@ __device__ __forceinline__ int32_t wfa_pair_dispatch(const SeqView &q, const Seq
 // score steps are its critical path, so four warps share each step); when
 // that queue is empty each warp takes pairs of `shorts` on its own.  Ring
 // slots: one region of nslot * slot_width int32 per warp (team mode uses the
-// block's first).
+// block's first).  Five resident blocks per SM (96 registers, no spills) beat
+// four with more registers; six or more spill and run slower.
 template <int U>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
            int32_t *__restrict__ out, int32_t *__restrict__ scratch, int64_t slot_width,
            int *err_flag, int64_t *work, int64_t *hist)
