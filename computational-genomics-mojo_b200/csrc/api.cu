@@ -855,12 +855,14 @@ static int ensure_len32(gb2_ctx *c, size_t bytes)
 // Chunked host-to-device pipeline.  For each chunk the host scans the
 // chunk's offsets and lengths (while the GPU copies and aligns earlier
 // chunks), copies the word range the chunk touches plus its lengths (int32,
-// offsets rebuilt on the device, when the chunk is contiguous; else int64
-// offsets and lengths) and bands on the copy stream, and runs the chunk on
-// one of the context's two executors (alternating, so one chunk's kernels can
-// fill the GPU while the previous chunk's last blocks drain); results come
-// back on the executor's stream.  kPipeSets chunks are in flight: the copies
-// of a chunk wait on the device for the chunk that last used its buffers.  On any error every stream is drained before returning, so no copy
+// offsets rebuilt on the device by two small kernels on a stream of their
+// own, when the chunk is contiguous; else int64 offsets and lengths) and
+// bands on the copy stream, and runs the chunk on one of the context's two
+// executors (alternating, so one chunk's kernels can fill the GPU while the
+// previous chunk's last blocks drain); results come back on a separate
+// stream, so an executor's stream holds nothing but alignment kernels.
+// kPipeSets chunks are in flight: the copies of a chunk wait on the device for
+// the chunk that last used its buffers.  On any error every stream is drained before returning, so no copy
 // touches the caller's memory after the call.
 template <typename RunChunk>
 static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const int32_t *bands,
@@ -952,17 +954,21 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
         if (bands && (r = h2d(c, ps.bands.p, bands + p0, (size_t)m * 4, c->st_copy)))
             return r;
         CU(c, cudaEventRecord(ps.copied, c->st_copy));
-        CU(c, cudaStreamWaitEvent(x.st, ps.copied, 0));
-        if (cs.dense) {
+        if (cs.dense) {  // rebuild the offsets beside the executors, off the copy stream
+            CU(c, cudaStreamWaitEvent(c->st_prep, ps.copied, 0));
             const int32_t *d32 = (const int32_t *)ps.len32.p;
             int64_t *sums = (int64_t *)((char *)ps.len32.p + (size_t)m * 8);
             const int tiles = (int)((m + kExpandTile - 1) / kExpandTile);
-            k_expand_sums<<<tiles, 256, 0, x.st>>>(m, d32, d32 + m, sums);
-            k_expand_write<<<tiles, 256, 0, x.st>>>(m, d32, d32 + m, sums, cs.qw0, cs.rw0,
-                                                    (int64_t *)ps.qo.p, (int64_t *)ps.ql.p,
-                                                    (int64_t *)ps.ro.p, (int64_t *)ps.rl.p);
+            k_expand_sums<<<tiles, 256, 0, c->st_prep>>>(m, d32, d32 + m, sums);
+            k_expand_write<<<tiles, 256, 0, c->st_prep>>>(m, d32, d32 + m, sums, cs.qw0, cs.rw0,
+                                                          (int64_t *)ps.qo.p, (int64_t *)ps.ql.p,
+                                                          (int64_t *)ps.ro.p, (int64_t *)ps.rl.p);
             CU(c, cudaGetLastError());
             c->launches += 2;
+            CU(c, cudaEventRecord(ps.ready, c->st_prep));
+            CU(c, cudaStreamWaitEvent(x.st, ps.ready, 0));
+        } else {
+            CU(c, cudaStreamWaitEvent(x.st, ps.copied, 0));
         }
         const SeqView qv{(const uint64_t *)ps.qw.p, (const int64_t *)ps.qo.p,
                          (const int64_t *)ps.ql.p, cs.qw0, qn};
@@ -974,20 +980,25 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
             return r;
         void *dst = out_pinned ? (char *)out_host + p0 * out_elem
                                : (char *)c->pin_out + p0 * out_elem;
-        CU(c, cudaMemcpyAsync(dst, ps.out.p, (size_t)m * out_elem, cudaMemcpyDeviceToHost, x.st));
-        CU(c, cudaEventRecord(ps.done, x.st));
+        // results return on their own stream, so the executor's next chunk does not
+        // wait for this copy
+        CU(c, cudaEventRecord(ps.kern, x.st));
+        CU(c, cudaStreamWaitEvent(c->st_back, ps.kern, 0));
+        CU(c, cudaMemcpyAsync(dst, ps.out.p, (size_t)m * out_elem, cudaMemcpyDeviceToHost,
+                              c->st_back));
+        CU(c, cudaEventRecord(ps.done, c->st_back));
         return GB2_OK;
     };
     for (int64_t ci = 0; ci < nchunks && !rc; ++ci)
         rc = issue(ci);
     if (rc) {
-        cudaStreamSynchronize(c->st_copy);
-        cudaStreamSynchronize(c->x.st);
-        cudaStreamSynchronize(c->x2.st);
+        for (cudaStream_t st : {c->st_copy, c->st_prep, c->x.st, c->x2.st, c->st_back})
+            cudaStreamSynchronize(st);
         cudaGetLastError();
         return rc;
     }
     CU(c, cudaStreamSynchronize(c->x2.st));
+    CU(c, cudaStreamSynchronize(c->st_back));
     if ((rc = sync_and_check(c)))
         return rc;
     if (!out_pinned)
@@ -1043,6 +1054,8 @@ int gb2_create(int device, gb2_ctx **out)
     c->sm_count = prop.multiProcessorCount;
     bool ok = exec_init(c->x) == GB2_OK && exec_init(c->x2) == GB2_OK &&
               cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->st_prep, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->st_back, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
     for (int i = 0; ok && i < 2; ++i) {
         ok = cudaMallocHost(&c->pin[i], (size_t)kPinChunk) == cudaSuccess &&
@@ -1053,11 +1066,11 @@ int gb2_create(int device, gb2_ctx **out)
     for (int i = 0; ok && i < kResidentParts; ++i)
         ok = cudaEventCreateWithFlags(&c->kdone[i], cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < kPipeSets; ++i) {
-        ok = cudaEventCreateWithFlags(&c->pipe[i].copied, cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&c->pipe[i].done, cudaEventDisableTiming) == cudaSuccess;
-        if (ok) {
-            cudaEventRecord(c->pipe[i].copied, c->x.st);
-            cudaEventRecord(c->pipe[i].done, c->x.st);
+        PipeSet &ps = c->pipe[i];
+        for (cudaEvent_t *e : {&ps.copied, &ps.ready, &ps.kern, &ps.done}) {
+            ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+            if (ok)
+                cudaEventRecord(*e, c->x.st);
         }
     }
     if (!ok) {
@@ -1074,10 +1087,9 @@ int gb2_destroy(gb2_ctx *c)
     if (!c)
         return GB2_EINVAL;
     cudaSetDevice(c->device);
-    if (c->st_copy)
-        cudaStreamSynchronize(c->st_copy);
-    if (c->x.st)
-        cudaStreamSynchronize(c->x.st);
+    for (cudaStream_t st : {c->st_copy, c->st_prep, c->st_back, c->x.st, c->x2.st})
+        if (st)
+            cudaStreamSynchronize(st);
     harvest_profile(c);
     exec_free(c->x);
     exec_free(c->x2);
@@ -1096,10 +1108,9 @@ int gb2_destroy(gb2_ctx *c)
         for (DevBuf *b : pb)
             if (b->p)
                 cudaFree(b->p);
-        if (ps.copied)
-            cudaEventDestroy(ps.copied);
-        if (ps.done)
-            cudaEventDestroy(ps.done);
+        for (cudaEvent_t e : {ps.copied, ps.ready, ps.kern, ps.done})
+            if (e)
+                cudaEventDestroy(e);
     }
     for (int i = 0; i < kResidentParts; ++i)
         if (c->kdone[i])
@@ -1118,8 +1129,9 @@ int gb2_destroy(gb2_ctx *c)
         cudaEventDestroy(c->t0);
     if (c->t1)
         cudaEventDestroy(c->t1);
-    if (c->st_copy)
-        cudaStreamDestroy(c->st_copy);
+    for (cudaStream_t st : {c->st_copy, c->st_prep, c->st_back})
+        if (st)
+            cudaStreamDestroy(st);
     delete c;
     return GB2_OK;
 }
@@ -1130,8 +1142,8 @@ int gb2_sync(gb2_ctx *c)
         return GB2_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    CU(c, cudaStreamSynchronize(c->st_copy));
-    CU(c, cudaStreamSynchronize(c->x2.st));
+    for (cudaStream_t st : {c->st_copy, c->st_prep, c->st_back, c->x2.st})
+        CU(c, cudaStreamSynchronize(st));
     return sync_and_check(c);
 }
 

@@ -44,9 +44,11 @@ constexpr int64_t kCigarArenaCap = 16ll << 30;  // WFA history arena, bytes at m
 // One set of device buffers of the end-to-end pipeline.
 struct PipeSet {
     DevBuf qw, rw, qo, ql, ro, rl, bands, out, len32;
-    cudaEvent_t copied = nullptr, done = nullptr;
+    // copied: inputs on the device; ready: offsets rebuilt (contiguous chunks);
+    // kern: the chunk's kernels ended; done: its results are back on the host
+    cudaEvent_t copied = nullptr, ready = nullptr, kern = nullptr, done = nullptr;
 };
-constexpr int kPipeSets = 3;  // chunks in flight in the host pipeline
+constexpr int kPipeSets = 6;  // chunks in flight in the host pipeline
 constexpr int64_t kResidentSplit = 1 << 18;  // resident SW batches this large run in parts
 constexpr int kResidentParts = 4;
 
@@ -84,6 +86,8 @@ struct gb2_ctx {
     gb2::Exec x;                  // the executor of the blocking entry points
     gb2::Exec x2;                 // second executor: the host pipeline alternates chunks
     cudaStream_t st_copy = nullptr;
+    cudaStream_t st_prep = nullptr;  // host pipeline: offset rebuild of contiguous chunks
+    cudaStream_t st_back = nullptr;  // host pipeline: result copies to the host
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::mutex mu;                // serialises the entry points of this context
     std::mutex err_mu;
