@@ -53,9 +53,11 @@ SCORING = (2, -4, -4, -2)
 BAND = 32
 SW_OPS_PER_CELL = 11  # int32 ops per cell of the reference recurrence (align_cpu.mojo:270-296)
 SW_OPS_PER_CELL_PACKED = 5.5  # the same ops on int16x2 lanes: two cells per lane-op
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel on
-# this workload, from the ncu capture summarised in profiles/sw_pack16_kernel_b32_1M_reads.md
-SW_PACKED_TRAFFIC_BYTES = 136.1e6
+# dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel per step of this
+# workload: a step runs as 4 launches of 262,144 pairs; one captured launch read 32.02 MB
+# and wrote 0 B (its 3.1 MB of results were still in L2 when it ended), times 4.  From the
+# ncu capture summarised in profiles/sw_pack16_kernel_b32_1M_reads.md
+SW_PACKED_TRAFFIC_BYTES = 128.1e6
 
 
 def parse():
@@ -376,7 +378,7 @@ def our_arm(args, dist: Dist):
                          "peak_source": "gb2_int_peak microkernels in this run: "
                                         "max(IADD, IMNMX, 2 x DPX viaddmax) lane-ops/s",
                          "traffic": SW_PACKED_TRAFFIC_BYTES if packed else None,
-                         "traffic_unit": "bytes per launch (ncu)",
+                         "traffic_unit": "bytes per step, 4 launches (ncu)",
                          "hbm": {"achieved": round(alg_bytes / (kernel_ms * 1e-3) / 1e9, 2),
                                  "peak": hbm_peak, "unit": "GB/s",
                                  "frac": round(alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, 5),
