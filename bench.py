@@ -351,8 +351,12 @@ def our_arm(args, dist: Dist):
         if args.gpus == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             g, n, dt = cpu_sw_gcups(q, r, args.cpu_sample, threads)
+            g1, n1, dt1 = cpu_sw_gcups(q, r, max(1000, args.cpu_sample // 5), 1)
             cpu = {"value": round(g, 4), "unit": "GCUPS", "cores": threads, "kind": "port",
-                   "sample": f"first {n} pairs of the workload ({dt:.1f} s)"}
+                   "sample": f"first {n} pairs of the workload ({dt:.1f} s)",
+                   "single_thread": {"value": round(g1, 4), "unit": "GCUPS", "cores": 1,
+                                     "sample": f"first {n1} pairs ({dt1:.1f} s), the "
+                                               "reference's serial loop"}}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "GCUPS",
             "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
@@ -362,7 +366,9 @@ def our_arm(args, dist: Dist):
                        "query_bp": 150, "target_bp": 200, "scoring": list(SCORING),
                        "path": "batched" if batched else "plain", "variant": args.variant,
                        "l2": "flushed between timed steps (256 MB device write)",
-                       "cells_per_step_per_gpu": cells},
+                       "cells_per_step_per_gpu": cells,
+                       "generator": synth.GENERATOR, "seed": hex(seed),
+                       "seed_rule": "0xb2000001 + 7919 * rank"},
             "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GCUPS",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
@@ -390,7 +396,8 @@ def our_arm(args, dist: Dist):
     dq.close()
     dr.close()
     if line is not None and dist.world == 1 and not args.no_extras:
-        line["extras"] = extras(args, dev, line["roofline"]["peak"])
+        line["extras"] = extras(args, dev, line["roofline"]["peak"],
+                                line["roofline"]["hbm"]["peak"])
     dev.close()
     dist.close()
     if line:
@@ -411,7 +418,7 @@ def _time_steps(dev, fn, steps, warmup):
     return statistics.median(ts)
 
 
-def extras(args, dev, peak_ops):
+def extras(args, dev, peak_ops, hbm_peak):
     """Batched queue vs plain launch vs per-call drop-in on the mixed-length workloads,
     with the CPU restatement of the reference beside each (all host threads)."""
     import oracle as O
@@ -466,6 +473,10 @@ def extras(args, dev, peak_ops):
     tb = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True), 2, 1)
     wcells = dev.stats()["work_units"] // 3
     tp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False), 2, 1)
+    w200 = WFAConfig(4, 6, 2, 200)
+    t200 = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, w200, batched=True), 2, 1)
+    c200 = dev.wfa_affine(dq, dr, w200, batched=True)
+    wbytes = q.packed.nbytes + r.packed.nbytes + 20 * n
     qp, _, qo, ql = q.arrays()
     rp, _, ro, rl = r.arrays()
     m = 300
@@ -496,7 +507,17 @@ def extras(args, dev, peak_ops):
                      "ops_per_cell": 13,
                      "achieved": round(wcells * 13 / (tb * 1e-3) / 1e9, 1),
                      "peak": peak_ops, "unit": "Gop/s",
-                     "frac": round(wcells * 13 / (tb * 1e-3) / 1e9 / peak_ops, 4)},
+                     "frac": round(wcells * 13 / (tb * 1e-3) / 1e9 / peak_ops, 4),
+                     # bytes: both sequences' packed words + 20 B of offsets, lengths
+                     # and the cost per pair
+                     "hbm": {"bytes": int(wbytes),
+                             "achieved": round(wbytes / (tb * 1e-3) / 1e9, 2),
+                             "peak": hbm_peak, "unit": "GB/s",
+                             "frac": round(wbytes / (tb * 1e-3) / 1e9 / hbm_peak, 6)}},
+        "max_error_200": {"pairs_per_s": round(n / (t200 * 1e-3), 1), "ms": round(t200, 3),
+                          "pairs_minus_one": int((c200 < 0).sum()),
+                          "note": "the reference's default budget: most long pairs exceed "
+                                  "it and return -1"},
     }
     # WFA with CIGAR traceback: the first 20,000 pairs of the same workload
     nc = 20_000

@@ -57,6 +57,11 @@ def _copy(ptr, n, dtype):
     return np.frombuffer(buf, dtype, count=n).copy()
 
 
+# Generator of every synthetic workload (csrc/synth.c): a SplitMix64-seeded xoshiro256**
+# stream per workload; bump the version when its output for a given seed changes.
+GENERATOR = "genomics_synth v1 (SplitMix64-seeded xoshiro256**)"
+
+
 def default_seed(workload: int) -> int:
     return 0xB2000000 + int(workload)
 
