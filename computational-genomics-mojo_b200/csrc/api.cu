@@ -526,6 +526,22 @@ int wfa_begin(gb2_ctx *c, Exec &x)
     return GB2_OK;
 }
 
+// Warps per block of the WFA kernel.  A batch of at most kWfaWideMaxPairs pairs (a
+// request group of the server, a small call) that holds pairs of at least
+// kWfaWideTeamLen bases runs the wide kernel: one 16-warp block per SM, each
+// of those pairs aligned by a whole block, the rest one per warp.  A long
+// pair's score steps are its critical path, so four times the threads per
+// step cut a small batch's latency; large batches keep the 4-warp blocks,
+// whose throughput is higher.
+constexpr int64_t kWfaWideMaxPairs = 2048;
+constexpr int64_t kWfaWideTeamLen = 8192;
+static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
+{
+    if (variant & 0xff)
+        return 4;  // the tuning variants are 4-warp kernels
+    return n <= kWfaWideMaxPairs && std::max(qmax, rmax) >= kWfaWideTeamLen ? kWfaWideWarps : 4;
+}
+
 int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
              const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags, int64_t *d_hist)
 {
@@ -544,13 +560,14 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     // choice, bit 6 = no pair aligned by a whole block, bit 7 = every pair of
     // at least kWfaTeamMinLen bases aligned by a whole block.
     const int variant = (flags >> 8) & 0xff;
+    const int bw = wfa_block_warps(qmax, rmax, n, variant);
     const int64_t warp_bytes = (int64_t)nslot * slot_width * 4;
-    int64_t grid =
-        (int64_t)c->sm_count * ((variant & 15) ? (variant & 15) : wfa_blocks_per_sm(variant));
-    grid = std::min(grid, std::max<int64_t>(c->sm_count, kWfaScratchCap / (4 * warp_bytes)));
-    grid = std::min(grid, std::max<int64_t>(1, (n + 3) / 4));
+    int64_t grid = (int64_t)c->sm_count *
+                   ((variant & 15) ? (variant & 15) : wfa_blocks_per_sm(variant, bw));
+    grid = std::min(grid, std::max<int64_t>(c->sm_count, kWfaScratchCap / (bw * warp_bytes)));
+    grid = std::min(grid, std::max<int64_t>(1, bw == 4 ? (n + 3) / 4 : n));
     int rc;
-    if ((rc = ensure(c, x.scratch32, (size_t)(grid * 4 * warp_bytes), x.st)) ||
+    if ((rc = ensure(c, x.scratch32, (size_t)(grid * bw * warp_bytes), x.st)) ||
         (rc = ensure(c, x.counters, kCounterBytes, x.st)))
         return rc;
     CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
@@ -559,8 +576,11 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     PairList shorts{nullptr, n, nullptr, ctr};
     if (flags & GB2_FLAG_BATCHED) {
         const int nb = kLenBuckets;
-        // one pair per block for the longest pairs, one wave of blocks of them
-        const int64_t team_pairs = (variant & 0x40) ? 0 : (variant & 0x80) ? n : grid;
+        // one pair per block for the longest pairs: one wave of blocks of them, or
+        // with the wide kernel every pair of at least kWfaWideTeamLen bases
+        const int64_t team_pairs =
+            (variant & 0x40) ? 0 : ((variant & 0x80) || bw != 4) ? n : grid;
+        const int64_t team_len = bw != 4 ? kWfaWideTeamLen : kWfaTeamMinLen;
         if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
             (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
             (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) ||
@@ -572,8 +592,7 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
         k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, (int32_t *)x.keys.p,
                                                   (int *)x.counts.p);
         k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, nb, seg);
-        k_split_wfa<<<1, 1, 0, x.st>>>((const int *)x.counts.p, n, kWfaTeamMinLen, team_pairs,
-                                       seg);
+        k_split_wfa<<<1, 1, 0, x.st>>>((const int *)x.counts.p, n, team_len, team_pairs, seg);
         k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
                                              (int32_t *)x.queue.p);
         CU(c, cudaGetLastError());
@@ -583,7 +602,7 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
         shorts = PairList{qd, 0, seg + 2, ctr};
     }
     cudaEvent_t e0 = prof_begin(c, x.st);
-    CU(c, launch_wfa(variant, qv, rv, p, longs, shorts, d_out, (int32_t *)x.scratch32.p,
+    CU(c, launch_wfa(variant, bw, qv, rv, p, longs, shorts, d_out, (int32_t *)x.scratch32.p,
                      slot_width, (int)grid, (int *)x.errflag.p, (int64_t *)x.work.p, d_hist,
                      x.st));
     prof_end(c, e0, x.st);

@@ -86,17 +86,19 @@ struct WfaParams {
     int32_t x, o, e, max_error;
 };
 
-// WFA over two pair lists: `longs` one pair per 128-thread block, then
-// `shorts` one pair per warp.  scratch: grid * 4 regions of nslot *
-// slot_width int32.
-// Resident 128-thread blocks per SM of the WFA kernel variant.
-int wfa_blocks_per_sm(int variant);
+// WFA over two pair lists: `longs` one pair per block of block_warps warps
+// (4, or kWfaWideWarps for the wide kernel), then `shorts` one pair per warp.
+// scratch: grid * block_warps regions of nslot * slot_width int32.
+constexpr int kWfaWideWarps = 16;
+// Resident blocks per SM of the WFA kernel variant.
+int wfa_blocks_per_sm(int variant, int block_warps);
 // hist (optional): per pair, the bytes of the cell part of its WFA history
 // record (wfa_hist_cell_bytes summed over the visited scores), 0 when the
 // cost is -1.
-cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
-                       PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
-                       int grid, int *err_flag, int64_t *work, int64_t *hist, cudaStream_t st);
+cudaError_t launch_wfa(int variant, int block_warps, SeqView q, SeqView r, WfaParams p,
+                       PairList longs, PairList shorts, int32_t *out, int32_t *scratch,
+                       int64_t slot_width, int grid, int *err_flag, int64_t *work, int64_t *hist,
+                       cudaStream_t st);
 
 // WFA history record of one pair (the CIGAR traceback's input), at a 16-byte
 // aligned offset of an arena: int32 header[3 * S] (per visited score index:

@@ -135,7 +135,7 @@ extern "C" int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
     gb2::WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
     const gb2::PairList none{nullptr, 0, nullptr, counter};
     const gb2::PairList pl{nullptr, n_pairs, nullptr, counter};
-    if (gb2::launch_wfa(0, qv, rv, p, none, pl, out_cost, rings, slot_width, (int)blocks,
+    if (gb2::launch_wfa(0, 4, qv, rv, p, none, pl, out_cost, rings, slot_width, (int)blocks,
                         err_flag, nullptr, nullptr, st) != cudaSuccess) {
         cudaGetLastError();
         return GB2_ECUDA;

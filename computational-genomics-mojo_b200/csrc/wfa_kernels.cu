@@ -544,19 +544,23 @@ __device__ __forceinline__ int32_t wfa_pair_dispatch(const SeqView &q, const Seq
 }
 
 // Persistent kernel over two length-sorted queues: every block first takes
-// pairs of `longs` one at a time as a team of its 4 warps (a long pair's
-// score steps are its critical path, so four warps share each step); when
-// that queue is empty each warp takes pairs of `shorts` on its own.  Ring
+// pairs of `longs` one at a time as a team of its BW warps (a long pair's
+// score steps are its critical path, so the block's warps share each step);
+// when that queue is empty each warp takes pairs of `shorts` on its own.  Ring
 // slots: one region of nslot * slot_width int32 per warp (team mode uses the
-// block's first).  Five resident blocks per SM (96 registers, no spills) beat
-// four with more registers; six or more spill and run slower.
-template <int U>
-__global__ void __launch_bounds__(128, 5)
+// block's first).  Shared memory (dynamic): per warp two sequence copies of
+// kWfaSeqWords words, BW * 4 * kWfaSeqWords uint32 in all.
+// BW = 4: five resident blocks per SM (96 registers, no spills) beat four with
+// more registers; six or more spill and run slower.  BW = 16: one 512-thread
+// block per SM, so each of the longest pairs gets a whole SM's 16 warps.
+template <int U, int BW>
+__global__ void __launch_bounds__(32 * BW, BW == 4 ? 5 : 1)
 wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
            int32_t *__restrict__ out, int32_t *__restrict__ scratch, int64_t slot_width,
            int *err_flag, int64_t *work, int64_t *hist)
 {
-    __shared__ __align__(16) uint32_t seqs[4 * 2 * 2 * kWfaSeqWords];
+    static_assert(BW >= 4, "team copies need 4 warps' share of shared memory");
+    extern __shared__ __align__(16) uint32_t seqs[];
     __shared__ int64_t team_slot;
     WfaShape w;
     w.g = gcd_i(p.x, gcd_i(p.o, p.e));
@@ -572,7 +576,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
     int64_t nl;
     const int32_t *__restrict__ lq = pairs_resolve(longs, nl);
     if (nl > 0) {
-        int32_t *const region = scratch + (int64_t)blockIdx.x * 4 * region_words;
+        int32_t *const region = scratch + (int64_t)blockIdx.x * BW * region_words;
         for (;;) {
             __syncthreads();
             if (threadIdx.x == 0)
@@ -582,7 +586,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
             if (si >= nl)
                 break;
             const int64_t pi = lq ? (int64_t)lq[si] : si;
-            wfa_pair_dispatch<U, 4>(q, r, p, w, pi, region, slot_width, seqs,
+            wfa_pair_dispatch<U, BW>(q, r, p, w, pi, region, slot_width, seqs,
                                     seqs + 2 * kWfaTeamSeqWords, kWfaTeamSeqWords, out, err_flag,
                                     work, hist);
         }
@@ -591,7 +595,7 @@ wfa_kernel(SeqView q, SeqView r, WfaParams p, PairList longs, PairList shorts,
 
     int64_t ns;
     const int32_t *__restrict__ sq = pairs_resolve(shorts, ns);
-    int32_t *const region = scratch + ((int64_t)blockIdx.x * 4 + wib) * region_words;
+    int32_t *const region = scratch + ((int64_t)blockIdx.x * BW + wib) * region_words;
     uint32_t *const my = seqs + wib * 4 * kWfaSeqWords;
     for (;;) {
         int64_t b0 = 0;
@@ -737,37 +741,67 @@ int wfa_cigar_blocks_per_sm()
     return nb > 0 ? nb : 1;
 }
 
-int wfa_blocks_per_sm(int variant)
+static size_t wfa_smem_bytes(int bw) { return (size_t)bw * 4 * kWfaSeqWords * 4; }
+
+// One-time opt-in to the kernel's dynamic shared memory (above 48 KB for BW = 16).
+template <int U, int BW>
+static void wfa_prepare()
 {
+    static const cudaError_t e = cudaFuncSetAttribute(
+        wfa_kernel<U, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfa_smem_bytes(BW));
+    (void)e;
+}
+
+template <int U, int BW>
+static int wfa_occupancy()
+{
+    wfa_prepare<U, BW>();
     int n = 0;
-    cudaError_t e;
-    if (variant & 0x20)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<1>, 128, 0);
-    else if (variant & 0x10)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<2>, 128, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<4>, 128, 0);
-    if (e != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wfa_kernel<U, BW>, 32 * BW,
+                                                      wfa_smem_bytes(BW)) != cudaSuccess) {
         cudaGetLastError();
-        return 4;
+        return BW == 4 ? 4 : 1;
     }
     return n > 0 ? n : 1;
 }
 
-cudaError_t launch_wfa(int variant, SeqView q, SeqView r, WfaParams p, PairList longs,
-                       PairList shorts, int32_t *out, int32_t *scratch, int64_t slot_width,
-                       int grid, int *err_flag, int64_t *work, int64_t *hist, cudaStream_t st)
+int wfa_blocks_per_sm(int variant, int block_warps)
 {
-    // variant bits 4-5: diagonals per thread per round 4 (default), 2 or 1
+    if (block_warps == kWfaWideWarps)
+        return wfa_occupancy<4, kWfaWideWarps>();
     if (variant & 0x20)
-        wfa_kernel<1><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work, hist);
-    else if (variant & 0x10)
-        wfa_kernel<2><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work, hist);
-    else
-        wfa_kernel<4><<<grid, 128, 0, st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
-                                            err_flag, work, hist);
+        return wfa_occupancy<1, 4>();
+    if (variant & 0x10)
+        return wfa_occupancy<2, 4>();
+    return wfa_occupancy<4, 4>();
+}
+
+cudaError_t launch_wfa(int variant, int block_warps, SeqView q, SeqView r, WfaParams p,
+                       PairList longs, PairList shorts, int32_t *out, int32_t *scratch,
+                       int64_t slot_width, int grid, int *err_flag, int64_t *work, int64_t *hist,
+                       cudaStream_t st)
+{
+    // block_warps kWfaWideWarps: the wide kernel (4 diagonals per thread per
+    // round); otherwise variant bits 4-5: diagonals per thread per round 4
+    // (default), 2 or 1
+    if (block_warps == kWfaWideWarps) {
+        wfa_prepare<4, kWfaWideWarps>();
+        wfa_kernel<4, kWfaWideWarps><<<grid, 32 * kWfaWideWarps, wfa_smem_bytes(kWfaWideWarps),
+                                       st>>>(q, r, p, longs, shorts, out, scratch, slot_width,
+                                             err_flag, work, hist);
+    } else if (variant & 0x20) {
+        wfa_prepare<1, 4>();
+        wfa_kernel<1, 4><<<grid, 128, wfa_smem_bytes(4), st>>>(
+            q, r, p, longs, shorts, out, scratch, slot_width, err_flag, work, hist);
+    } else if (variant & 0x10) {
+        wfa_prepare<2, 4>();
+        wfa_kernel<2, 4><<<grid, 128, wfa_smem_bytes(4), st>>>(
+            q, r, p, longs, shorts, out, scratch, slot_width, err_flag, work, hist);
+    } else {
+        wfa_prepare<4, 4>();
+        wfa_kernel<4, 4><<<grid, 128, wfa_smem_bytes(4), st>>>(
+            q, r, p, longs, shorts, out, scratch, slot_width, err_flag, work, hist);
+    }
     return cudaGetLastError();
 }
 
