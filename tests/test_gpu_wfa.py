@@ -135,7 +135,9 @@ def test_length_classes(device, oracle):
     """Pairs on both sides of the block-per-pair threshold (2,048 bases), of
     the per-warp and per-block shared-memory sequence copies (10,240 and
     41,056 bases), unrelated pairs whose diagonal interval grows to thousands,
-    and long pairs: batched, plain and tuning variants against the oracle."""
+    and long pairs: batched, plain and tuning variants against the oracle.
+    This batch (66 pairs, some of 8 kbp or more) runs the 16-warp kernel by
+    default; the tuning variants run the 4-warp kernel."""
     rng = random.Random(2024)
     qs, rs = [], []
     for _ in range(40):                       # around the threshold, narrow intervals
