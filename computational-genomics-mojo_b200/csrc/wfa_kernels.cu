@@ -413,7 +413,8 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
                             if (Mx)
                                 mx = (int32_t)Mx[kc];
                             const int32_t i0 = max(io, ie), d0 = max(dop, dex), m0 = mx + 1;
-                            const int32_t m1 = max(m0, max(i0 + 1, d0));
+                            // max(mx + 1, i0 + 1, d0) as two DPX add-max instructions
+                            const int32_t m1 = __viaddmax_s32(mx, 1, __viaddmax_s32(i0, 1, d0));
                             if (HREC) {
                                 // the traceback's tests (align_cpu.mojo:509-601), first
                                 // equal source: M from mismatch, I, D; I / D from an
@@ -448,7 +449,6 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
                                     hm_out[ks[u] - a] = mv[u];
                                     hd_out[ks[u] - a] = (uint8_t)dec[u];
                                 }
-                                hit |= ks[u] == target && mv[u] >= qlen;
                             }
                         }
                     };
@@ -457,6 +457,10 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
                         round(k0, std::integral_constant<int, U>{}, std::true_type{});
                     for (; k0 <= b; k0 += TW)
                         round(k0, std::integral_constant<int, 1>{}, std::false_type{});
+                    // the thread that owns the target diagonal reads back what it
+                    // stored there this step (its own store, so program order holds)
+                    if (target >= a && target <= b && ((target - a) & (TW - 1)) == tt)
+                        hit = (int32_t)Mw[target] >= qlen;
                     if (HREC)
                         hcur += wfa_hist_cell_bytes(b - a + 1) / 4;
                     // widen for the next step (see above); the positions
