@@ -461,6 +461,16 @@ def extras(args, dev, peak_ops, hbm_peak):
         "cpu_gcups": round(cpu_cells / tcpu / 1e9, 3), "cpu_cores": threads,
         "cpu_sample": f"first {ns} pairs",
     }
+    # autotuner: the register-kernel shape of each band class, tuned inside the
+    # whole mixed batch (one class after another), then the batch timed again
+    from genomics_b200 import autotune
+    table = autotune.tune(dev, dq, dr, sw_cfg=cfg, reps=3, pair_bands=bands)
+    tt = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=True), 3, 2)
+    out["mixed_sw_200k"]["autotuned"] = {
+        "table": table["sw"], "candidates_ms": table["measurements"],
+        "tuned_on": "the whole 200,000-pair mixed call, one band class after another",
+        "batched_gcups": round(cells / tt / 1e6, 2), "batched_ms": round(tt, 3)}
+    autotune.install(dev, {"sw": {str(b): 0 for b in autotune.SW_BANDS}})
     dq.close()
     dr.close()
     # long WFA: 100,000 pairs, 100-10,000 bp, 1-10% divergence, x4 o6 e2
@@ -575,8 +585,37 @@ def extras(args, dev, peak_ops, hbm_peak):
     drn.close()
     dq.close()
     dr.close()
+    out["graph_replay"] = graph_bench(dev)
     out["serving"] = serve_bench(dev)
     return out
+
+
+def graph_bench(dev, calls=200):
+    """Per-call host time of small resident batches, eager (the default) vs replayed
+    from a captured CUDA graph (GB2_FLAG_GRAPH): the first 2,000 pairs of the mixed-band SW
+    workload (planning kernels and four class launches per call) and 5,000 reads of
+    the default workload (one launch)."""
+    from genomics_b200 import AlignConfig, synth
+    from genomics_b200._lib import FLAG_GRAPH
+    res = {}
+    q3, r3, b3, _ = synth.generate(3, 2000)
+    q1, r1, _, _ = synth.generate(1, 5000)
+    for name, (q, r, bands) in (("mixed_sw_2000", (q3, r3, b3)), ("reads_5000", (q1, r1, None))):
+        cfg = AlignConfig(*SCORING, 32)
+        dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
+        row = {}
+        for mode, fl in (("eager_us", 0), ("graph_us", FLAG_GRAPH)):
+            for _ in range(3):
+                dev.sw_banded(dq, dr, cfg, bands=bands, flags=fl)
+            dev.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(calls):
+                dev.sw_banded(dq, dr, cfg, bands=bands, flags=fl)
+            row[mode] = round((time.perf_counter() - t0) / calls * 1e6, 1)
+        res[name] = row
+        dq.close()
+        dr.close()
+    return res
 
 
 def _slice(batch, i0, i1):

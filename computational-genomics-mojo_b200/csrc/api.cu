@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <thread>
 
 #include "runtime.cuh"
@@ -96,6 +97,7 @@ int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st)
     }
     size_t cap = std::max<size_t>(bytes, 256);
     cap = (cap + 255) & ~size_t(255);
+    ++c->buf_gen;  // captured graphs hold buffer addresses: they are stale now
     CU(c, cudaMalloc(&b.p, cap));
     b.cap = cap;
     return GB2_OK;
@@ -334,6 +336,13 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
     const bool force_literal = (flags & GB2_FLAG_GENERIC) != 0;
     const bool batched = (flags & GB2_FLAG_BATCHED) != 0;
     const int variant = (flags >> 8) & 0xff;  // tuning knob (G/K choice), 0 = default
+    // per band class: the caller's variant, else the one installed by the tuner
+    auto var_of = [&](int cls) -> int {
+        if (variant)
+            return variant;
+        const int slot = cls == 16 ? 0 : cls == 32 ? 1 : cls == 64 ? 2 : cls == 128 ? 3 : -1;
+        return slot >= 0 ? c->tune_sw[slot] : 0;
+    };
 
     // literal-kernel scratch (int64 rows), sized for the widest band
     const int64_t lit_stride = 3 * (2 * (int64_t)std::max(pi.max_band, 0) + 1);
@@ -359,11 +368,11 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
                 return rc;
             CU(c, cudaMemsetAsync(x.counters.p, 0, 64, x.st));
             pl.counter = (int *)x.counters.p;
-            grid = c->sm_count * sw_blocks_per_sm(cls, variant);
+            grid = c->sm_count * sw_blocks_per_sm(cls, var_of(cls));
         }
         cudaEvent_t e0 = profile ? prof_begin(c, x.st) : nullptr;
         if (cls > 0) {
-            CU(c, launch_sw(cls, variant, qv, rv, p, cfg->band_width, nullptr, pl, d_out, nullptr,
+            CU(c, launch_sw(cls, var_of(cls), qv, rv, p, cfg->band_width, nullptr, pl, d_out, nullptr,
                             0, grid, x.st));
         } else {
             const int rc = ensure_lit();
@@ -436,9 +445,9 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
         PairList pl{(const int32_t *)x.queue.p, 0, (const int64_t *)x.seg.p + 2 * k,
                     (int *)x.counters.p + kCounterStride * k};
         if (k != 4) {
-            const int grid = c->sm_count * sw_blocks_per_sm(cls_band[k], variant);
-            CU(c, launch_sw(cls_band[k], variant, qv, rv, p, cfg->band_width, d_bands, pl, d_out,
-                            nullptr, 0, grid, s));
+            const int grid = c->sm_count * sw_blocks_per_sm(cls_band[k], var_of(cls_band[k]));
+            CU(c, launch_sw(cls_band[k], var_of(cls_band[k]), qv, rv, p, cfg->band_width, d_bands,
+                            pl, d_out, nullptr, 0, grid, s));
         } else {
             CU(c, launch_sw(0, 0, qv, rv, p, cfg->band_width, d_bands, pl, d_out,
                             (int64_t *)x.scratch64.p, lit_stride, lit_grid, s));
@@ -559,8 +568,10 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     // flags bits 8-15: low 4 bits = blocks per SM, bits 4-5 = kernel unroll
     // choice, bit 6 = no pair aligned by a whole block, bit 7 = every pair of
     // at least kWfaTeamMinLen bases aligned by a whole block.
-    const int variant = (flags >> 8) & 0xff;
-    const int bw = wfa_block_warps(qmax, rmax, n, variant);
+    const int fvar = (flags >> 8) & 0xff;
+    const int bw = wfa_block_warps(qmax, rmax, n, fvar);
+    // the caller's variant, else (4-warp kernel) the one installed by the tuner
+    const int variant = fvar ? fvar : (bw == 4 ? c->tune_wfa : 0);
     const int64_t warp_bytes = (int64_t)nslot * slot_width * 4;
     int64_t grid = (int64_t)c->sm_count *
                    ((variant & 15) ? (variant & 15) : wfa_blocks_per_sm(variant, bw));
@@ -638,6 +649,113 @@ static int sync_and_check(gb2_ctx *c)
     CU(c, cudaStreamSynchronize(c->x.st));
     harvest_profile(c);
     return GB2_OK;
+}
+
+// Runs a resident call's device work on c->x.st, eagerly or, with
+// GB2_FLAG_GRAPH, through the context's replay cache g (GraphCache): the
+// first call with a key runs eagerly, the second is captured into a CUDA
+// graph, later ones launch it.  Eager is the default: each call here is one
+// to five persistent launches, and replaying them from a graph measured 6-10%
+// slower per call than launching them (2,000 mixed-band pairs: 3.04 vs
+// 2.75 ms; 5,000 reads: 164 vs 155 us).
+// issue(capturing) enqueues the work, joins every other stream it forks back
+// into c->x.st, and writes to the host only by cudaMemcpyAsync into the
+// pinned array at `host` (nullptr: no host copies in the work).  While
+// profiling is on, calls run eagerly: the kernel spans need events between
+// the launches, which a graph does not hold.  A capture that fails (an
+// unexpected reallocation, an unsupported call) leaves the key eager.
+template <typename Issue>
+static int run_graphed(gb2_ctx *c, GraphCache &g, const std::vector<int64_t> &key, int flags,
+                       char *host, Issue issue)
+{
+    if (!(flags & GB2_FLAG_GRAPH) || c->profiling.load())
+        return issue(false);
+    if (g.key != key || g.gen != c->buf_gen) {  // first call with this shape
+        g.reset();
+        g.key = key;
+        const int rc = issue(false);
+        g.gen = c->buf_gen;  // the call's own allocations belong to the shape
+        return rc;
+    }
+    if (g.failed)
+        return issue(false);
+    if (!g.exec) {
+        const int64_t l0 = c->launches.load();
+        cudaGraph_t graph = nullptr;
+        int rc = GB2_ECUDA;
+        if (cudaStreamBeginCapture(c->x.st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            rc = issue(true);
+            if (cudaStreamEndCapture(c->x.st, &graph) != cudaSuccess && rc == GB2_OK)
+                rc = GB2_ECUDA;
+        }
+        c->launches = l0;
+        bool ok = rc == GB2_OK && graph && c->buf_gen == g.gen &&
+                  cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+        if (ok) {
+            size_t nn = 0;
+            ok = cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess;
+            std::vector<cudaGraphNode_t> nodes(nn);
+            ok = ok && cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess;
+            for (size_t i = 0; ok && i < nn; ++i) {
+                cudaGraphNodeType t;
+                ok = cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess;
+                if (ok && t == cudaGraphNodeTypeKernel) {
+                    ++g.kernels;
+                } else if (ok && t == cudaGraphNodeTypeMemcpy) {
+                    cudaMemcpy3DParms mp{};
+                    ok = cudaGraphMemcpyNodeGetParams(nodes[i], &mp) == cudaSuccess;
+                    const char *dst = (const char *)mp.dstPtr.ptr;
+                    ok = ok && host && mp.kind == cudaMemcpyDeviceToHost && dst >= host &&
+                         mp.extent.height <= 1 && mp.extent.depth <= 1;
+                    if (ok)
+                        g.copies.push_back(GraphCache::Copy{nodes[i], (size_t)(dst - host),
+                                                            mp.extent.width, mp.srcPtr.ptr});
+                }
+            }
+        }
+        if (!ok) {
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+            if (graph)
+                cudaGraphDestroy(graph);
+            g.exec = nullptr;
+            g.copies.clear();
+            g.kernels = 0;
+            g.failed = true;
+            cudaGetLastError();
+            return issue(false);
+        }
+        g.graph = graph;
+        g.host = host;
+    }
+    if (host != g.host) {  // the caller's result array moved: retarget the copies
+        for (const GraphCache::Copy &cp : g.copies)
+            if (cudaGraphExecMemcpyNodeSetParams1D(g.exec, cp.node, host + cp.dst_off, cp.src,
+                                                    cp.bytes, cudaMemcpyDeviceToHost) !=
+                cudaSuccess) {
+                g.reset();
+                cudaGetLastError();
+                return issue(false);
+            }
+        g.host = host;
+    }
+    CU(c, cudaGraphLaunch(g.exec, c->x.st));
+    c->launches += g.kernels;
+    return GB2_OK;
+}
+
+// The shape of a resident call over batches q and r, for GraphCache keys.
+static void key_batches(std::vector<int64_t> &k, const gb2_batch *q, const gb2_batch *r)
+{
+    for (const gb2_batch *b : {q, r}) {
+        k.push_back((int64_t)(uintptr_t)b->d_packed);
+        k.push_back((int64_t)(uintptr_t)b->d_offsets);
+        k.push_back((int64_t)(uintptr_t)b->d_lengths);
+        k.push_back(b->count);
+        k.push_back(b->n_words);
+        k.push_back(b->max_len);
+        k.push_back(b->min_len);
+    }
 }
 
 // Pinned host staging for results.
@@ -1084,6 +1202,7 @@ int gb2_create(int device, gb2_ctx **out)
     }
     for (int i = 0; ok && i < kResidentParts; ++i)
         ok = cudaEventCreateWithFlags(&c->kdone[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < kPipeSets; ++i) {
         PipeSet &ps = c->pipe[i];
         for (cudaEvent_t *e : {&ps.copied, &ps.ready, &ps.kern, &ps.done}) {
@@ -1110,6 +1229,8 @@ int gb2_destroy(gb2_ctx *c)
         if (st)
             cudaStreamSynchronize(st);
     harvest_profile(c);
+    c->g_sw.reset();
+    c->g_wfa.reset();
     exec_free(c->x);
     exec_free(c->x2);
     CigarBufs &cb = c->cig;
@@ -1134,6 +1255,8 @@ int gb2_destroy(gb2_ctx *c)
     for (int i = 0; i < kResidentParts; ++i)
         if (c->kdone[i])
             cudaEventDestroy(c->kdone[i]);
+    if (c->ev_join2)
+        cudaEventDestroy(c->ev_join2);
     for (int i = 0; i < 2; ++i) {
         if (c->pin[i])
             cudaFreeHost(c->pin[i]);
@@ -1302,10 +1425,19 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
     // Large batches run as kResidentParts parts alternating between the two
     // executors, each part's results copied back while the next part computes.
     const int parts = n >= kResidentSplit ? kResidentParts : 1;
+    std::vector<int64_t> key{1};
+    key_batches(key, q, r);
+    key.insert(key.end(), {cfg->match_score, cfg->mismatch, cfg->gap_open, cfg->gap_extend,
+                           cfg->band_width, n, flags, bands ? 1 : 0, pi.max_band});
     if (parts == 1) {
-        if ((rc = sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands,
-                          pi, n, (gb2_sw_result *)c->out_sw.p, flags)))
+        rc = run_graphed(c, c->g_sw, key, flags, nullptr, [&](bool capturing) -> int {
+            return sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg,
+                           d_bands, pi, n, (gb2_sw_result *)c->out_sw.p, flags, !capturing);
+        });
+        if (rc) {
+            cudaStreamSynchronize(c->x.st);
             return rc;
+        }
         return d2h_results(c, out, c->out_sw.p, (size_t)n * sizeof(gb2_sw_result));
     }
     const bool out_pinned = is_pinned(out);
@@ -1313,36 +1445,45 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
         return rc;
     gb2_sw_result *const host = out_pinned ? out : (gb2_sw_result *)c->pin_out;
     gb2_sw_result *const dres = (gb2_sw_result *)c->out_sw.p;
-    CU(c, cudaEventRecord(c->x.ev_fork, c->x.st));  // bands copied before either executor runs
-    CU(c, cudaStreamWaitEvent(c->x2.st, c->x.ev_fork, 0));
-    // profiling: one span per call, from the first part's start to the later of
-    // the two executors' last kernels (the parts overlap, so their own
-    // durations would double-count)
-    cudaEvent_t span0 = prof_begin(c, c->x.st);
-    const int64_t per = (n + parts - 1) / parts;
-    for (int k = 0; k < parts && rc == GB2_OK; ++k) {
-        const int64_t p0 = k * per, m = std::min(per, n - p0);
-        Exec &ex = (k & 1) ? c->x2 : c->x;
-        SeqView qv = view_of(q), rv = view_of(r);
-        qv.offsets += p0;
-        qv.lengths += p0;
-        rv.offsets += p0;
-        rv.lengths += p0;
-        rc = sw_core(c, ex, qv, rv, q->max_len, r->max_len, cfg, d_bands ? d_bands + p0 : nullptr,
-                     pi, m, dres + p0, flags, false);
-        if (!rc && cudaEventRecord(c->kdone[k], ex.st) != cudaSuccess)
-            rc = set_err(c, GB2_ECUDA, "event record failed");
-        if (!rc && cudaMemcpyAsync(host + p0, dres + p0, (size_t)m * sizeof(gb2_sw_result),
-                                   cudaMemcpyDeviceToHost, ex.st) != cudaSuccess)
-            rc = set_err(c, GB2_ECUDA, "result copy failed");
-    }
-    if (span0 && !rc) {
-        cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 2], 0);
-        cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 1], 0);
-        prof_end(c, span0, c->st_copy);
-    } else if (span0) {
-        cudaEventDestroy(span0);
-    }
+    auto issue = [&](bool capturing) -> int {
+        CU(c, cudaEventRecord(c->x.ev_fork, c->x.st));  // bands copied before either runs
+        CU(c, cudaStreamWaitEvent(c->x2.st, c->x.ev_fork, 0));
+        // profiling: one span per call, from the first part's start to the later
+        // of the two executors' last kernels (the parts overlap, so their own
+        // durations would double-count)
+        cudaEvent_t span0 = capturing ? nullptr : prof_begin(c, c->x.st);
+        const int64_t per = (n + parts - 1) / parts;
+        int r2 = GB2_OK;
+        for (int k = 0; k < parts && r2 == GB2_OK; ++k) {
+            const int64_t p0 = k * per, m = std::min(per, n - p0);
+            Exec &ex = (k & 1) ? c->x2 : c->x;
+            SeqView qv = view_of(q), rv = view_of(r);
+            qv.offsets += p0;
+            qv.lengths += p0;
+            rv.offsets += p0;
+            rv.lengths += p0;
+            r2 = sw_core(c, ex, qv, rv, q->max_len, r->max_len, cfg,
+                         d_bands ? d_bands + p0 : nullptr, pi, m, dres + p0, flags, false);
+            if (!r2 && !capturing && cudaEventRecord(c->kdone[k], ex.st) != cudaSuccess)
+                r2 = set_err(c, GB2_ECUDA, "event record failed");
+            if (!r2 && cudaMemcpyAsync(host + p0, dres + p0, (size_t)m * sizeof(gb2_sw_result),
+                                       cudaMemcpyDeviceToHost, ex.st) != cudaSuccess)
+                r2 = set_err(c, GB2_ECUDA, "result copy failed");
+        }
+        // the second executor joins the first (a captured graph must end there)
+        if (!r2 && (cudaEventRecord(c->ev_join2, c->x2.st) != cudaSuccess ||
+                    cudaStreamWaitEvent(c->x.st, c->ev_join2, 0) != cudaSuccess))
+            r2 = set_err(c, GB2_ECUDA, "joining the executors failed");
+        if (span0 && !r2) {
+            cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 2], 0);
+            cudaStreamWaitEvent(c->st_copy, c->kdone[parts - 1], 0);
+            prof_end(c, span0, c->st_copy);
+        } else if (span0) {
+            cudaEventDestroy(span0);
+        }
+        return r2;
+    };
+    rc = run_graphed(c, c->g_sw, key, flags, (char *)host, issue);
     const cudaError_t e2 = cudaStreamSynchronize(c->x2.st);
     const int rc2 = sync_and_check(c);
     if (rc)
@@ -1419,11 +1560,22 @@ int gb2_wfa_affine(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2
     int rc = wfa_validate(c, cfg, n);
     if (rc || n == 0)
         return rc;
-    if ((rc = ensure(c, c->out_wfa, (size_t)n * 4, c->x.st)) || (rc = wfa_begin(c, c->x)))
+    if ((rc = ensure(c, c->out_wfa, (size_t)n * 4, c->x.st)))
         return rc;
-    if ((rc = wfa_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, n,
-                       (int32_t *)c->out_wfa.p, flags)))
+    std::vector<int64_t> key{2};
+    key_batches(key, q, r);
+    key.insert(key.end(), {cfg->x, cfg->o, cfg->e, cfg->max_error, n, flags});
+    rc = run_graphed(c, c->g_wfa, key, flags, nullptr, [&](bool) -> int {
+        int r2;
+        if ((r2 = wfa_begin(c, c->x)))
+            return r2;
+        return wfa_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, n,
+                        (int32_t *)c->out_wfa.p, flags);
+    });
+    if (rc) {
+        cudaStreamSynchronize(c->x.st);
         return rc;
+    }
     if ((rc = wfa_end(c, c->x)))
         return rc;
     return d2h_results(c, out, c->out_wfa.p, (size_t)n * 4);
@@ -1530,6 +1682,195 @@ int gb2_stats(gb2_ctx *c, double *kernel_ms, int64_t *launches, int64_t *work_un
         *launches = c->launches.load();
     if (work_units)
         *work_units = c->work_units.load();
+    return GB2_OK;
+}
+
+// ---- autotuner ---------------------------------------------------------------
+int gb2_autotune(gb2_ctx *c, int kind, const gb2_batch *q, const gb2_batch *r, const void *cfgp,
+                 const int32_t *bands, int64_t n, int reps, gb2_tune_result *out)
+{
+    if (!c || !q || !r || !cfgp || !out)
+        return GB2_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    if (q->owner != c || r->owner != c)
+        return set_err(c, GB2_EINVAL, "batch belongs to another context");
+    if (n <= 0 || n > q->count || n > r->count)
+        return set_err(c, GB2_EINVAL, "n_pairs must be in [1, batch count]");
+    reps = std::max(1, std::min(reps, 50));
+    gb2_tune_result res{};
+    res.kind = kind;
+    std::vector<int> cand;
+    int *slot = nullptr;  // the table entry the winner goes to
+    size_t out_bytes = 0;
+    const void *d_res = nullptr;
+    std::function<int(int)> run;  // one run of a candidate on c->x, no host sync
+    SwPlanInfo pi;
+    int rc;
+    if (kind == GB2_TUNE_SW) {
+        const gb2_sw_cfg *cfg = (const gb2_sw_cfg *)cfgp;
+        res.band_class = classify_band(cfg->band_width);
+        switch (res.band_class) {
+        case 16: cand = {0, 1}; slot = &c->tune_sw[0]; break;
+        case 32: cand = {0, 1, 2}; slot = &c->tune_sw[1]; break;
+        case 64: cand = {0, 1}; slot = &c->tune_sw[2]; break;
+        case 128: cand = {0, 1}; slot = &c->tune_sw[3]; break;
+        default:
+            return set_err(c, GB2_EINVAL, "band %d has no kernel variants (16, 32, 64 or 128)",
+                           cfg->band_width);
+        }
+        if ((rc = sw_validate(c, cfg, bands, n, q->max_len, r->max_len, pi)))
+            return rc;
+        pi.narrow_lengths =
+            narrow_range(q->min_len, q->max_len) && narrow_range(r->min_len, r->max_len);
+        if (!pi.fast_ok)
+            return set_err(c, GB2_EINVAL, "these penalties take the literal kernel (no variants)");
+        out_bytes = (size_t)n * sizeof(gb2_sw_result);
+        if ((rc = ensure(c, c->out_sw, out_bytes, c->x.st)))
+            return rc;
+        const int32_t *d_bands = nullptr;
+        if (bands) {
+            if ((rc = ensure(c, c->bands, (size_t)n * 4, c->x.st)) ||
+                (rc = h2d(c, c->bands.p, bands, (size_t)n * 4, c->x.st)))
+                return rc;
+            d_bands = (const int32_t *)c->bands.p;
+        }
+        d_res = c->out_sw.p;
+        // the candidate goes into the table slot, so with per-pair bands the other
+        // classes of the mix run with their installed variants
+        run = [=](int v) {
+            *slot = v;
+            return sw_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, d_bands,
+                           pi, n, (gb2_sw_result *)c->out_sw.p, GB2_FLAG_BATCHED | GB2_FLAG_INT32,
+                           false);
+        };
+    } else if (kind == GB2_TUNE_WFA) {
+        const gb2_wfa_cfg *cfg = (const gb2_wfa_cfg *)cfgp;
+        if ((rc = wfa_validate(c, cfg, n)))
+            return rc;
+        // diagonals per thread per round 4, 2, 1 (bits 4-5); blocks per SM (bits 0-3)
+        cand = {0x00, 0x04, 0x03, 0x10, 0x20};
+        slot = &c->tune_wfa;
+        out_bytes = (size_t)n * 4;
+        if ((rc = ensure(c, c->out_wfa, out_bytes, c->x.st)))
+            return rc;
+        d_res = c->out_wfa.p;
+        run = [=](int v) {
+            int r2;
+            if ((r2 = wfa_begin(c, c->x)))
+                return r2;
+            return wfa_core(c, c->x, view_of(q), view_of(r), q->max_len, r->max_len, cfg, n,
+                            (int32_t *)c->out_wfa.p, GB2_FLAG_BATCHED | (v << 8));
+        };
+    } else {
+        return set_err(c, GB2_EINVAL, "kind must be GB2_TUNE_SW or GB2_TUNE_WFA");
+    }
+    // candidate 0 is the built-in choice, not whatever is installed now
+    const int saved = *slot;
+    *slot = 0;
+    auto finish = [&](int status) {
+        if (status != GB2_OK)
+            *slot = saved;
+        cudaStreamSynchronize(c->x.st);
+        return status;
+    };
+    auto settle = [&]() -> int {  // wait for the run; WFA reports its error flag
+        if (kind == GB2_TUNE_WFA)
+            return wfa_end(c, c->x);
+        CU(c, cudaStreamSynchronize(c->x.st));
+        return GB2_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        return finish(set_err(c, GB2_ECUDA, "creating timing events failed"));
+    }
+    std::vector<char> first(out_bytes), cur(out_bytes);
+    int best = cand[0];
+    float best_ms = 0.f;
+    rc = GB2_OK;
+    for (size_t i = 0; i < cand.size() && rc == GB2_OK; ++i) {
+        const int v = cand[i];
+        if ((rc = run(v)) || (rc = settle()))
+            break;
+        // results of every candidate equal the first's
+        if (cudaMemcpy(i ? cur.data() : first.data(), d_res, out_bytes, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+            rc = set_err(c, GB2_ECUDA, "reading back the results failed");
+            break;
+        }
+        if (i && memcmp(first.data(), cur.data(), out_bytes) != 0) {
+            rc = set_err(c, GB2_EKERNEL, "variant %#x gives other results than variant %#x", v,
+                         cand[0]);
+            break;
+        }
+        std::vector<float> t;
+        for (int k = 0; k < reps && rc == GB2_OK; ++k) {
+            float ms = 0.f;
+            if (cudaEventRecord(e0, c->x.st) != cudaSuccess || (rc = run(v)) ||
+                cudaEventRecord(e1, c->x.st) != cudaSuccess || (rc = settle()) ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                if (rc == GB2_OK)
+                    rc = set_err(c, GB2_ECUDA, "timing a variant failed");
+                break;
+            }
+            t.push_back(ms);
+        }
+        if (rc)
+            break;
+        std::sort(t.begin(), t.end());
+        const float med = t[t.size() / 2];
+        res.variant[res.n_candidates] = v;
+        res.ms[res.n_candidates] = med;
+        ++res.n_candidates;
+        if (i == 0 || med < best_ms) {
+            best = v;
+            best_ms = med;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc)
+        return finish(rc);
+    *slot = best;
+    res.chosen = best;
+    *out = res;
+    return finish(GB2_OK);
+}
+
+int gb2_tune_set(gb2_ctx *c, int kind, int band_class, int variant)
+{
+    if (!c || variant < 0 || variant > 0xff)
+        return GB2_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (kind == GB2_TUNE_WFA) {
+        c->tune_wfa = variant;
+        return GB2_OK;
+    }
+    const int slot = band_class == 16 ? 0 : band_class == 32 ? 1 : band_class == 64 ? 2
+                   : band_class == 128 ? 3 : -1;
+    if (kind != GB2_TUNE_SW || slot < 0)
+        return set_err(c, GB2_EINVAL, "no tuning entry for kind %d, band class %d", kind,
+                       band_class);
+    c->tune_sw[slot] = variant;
+    return GB2_OK;
+}
+
+int gb2_tune_get(gb2_ctx *c, int kind, int band_class, int *variant)
+{
+    if (!c || !variant)
+        return GB2_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (kind == GB2_TUNE_WFA) {
+        *variant = c->tune_wfa;
+        return GB2_OK;
+    }
+    const int slot = band_class == 16 ? 0 : band_class == 32 ? 1 : band_class == 64 ? 2
+                   : band_class == 128 ? 3 : -1;
+    if (kind != GB2_TUNE_SW || slot < 0)
+        return set_err(c, GB2_EINVAL, "no tuning entry for kind %d, band class %d", kind,
+                       band_class);
+    *variant = c->tune_sw[slot];
     return GB2_OK;
 }
 

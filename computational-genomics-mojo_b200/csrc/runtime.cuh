@@ -52,6 +52,45 @@ constexpr int kPipeSets = 6;  // chunks in flight in the host pipeline
 constexpr int64_t kResidentSplit = 1 << 18;  // resident SW batches this large run in parts
 constexpr int kResidentParts = 4;
 
+// Replay cache of one resident entry point (gb2_sw_banded, gb2_wfa_affine),
+// used with GB2_FLAG_GRAPH.  The device work of a call is captured into a CUDA graph on the second call in
+// a row with the same key -- everything the host decides the launches from:
+// the batches' device arrays and sizes, the scoring, n_pairs, flags -- and
+// while the context's buffers keep their addresses (gen), later calls with
+// that key launch the graph instead of re-issuing memsets, planning kernels,
+// the alignment kernels and the stream forks and joins one by one.  Result
+// copies to the caller's host array are memcpy nodes whose destination is
+// updated when the array moves.  Calls made while profiling is on run eagerly.
+struct GraphCache {
+    std::vector<int64_t> key;
+    uint64_t gen = 0;
+    bool failed = false;           // capture failed for this key: stay eager
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;           // kernel nodes, for the launch statistics
+    struct Copy {
+        cudaGraphNode_t node;
+        size_t dst_off, bytes;     // destination offset from the call's host base
+        const void *src;
+    };
+    std::vector<Copy> copies;
+    char *host = nullptr;          // host base the copy nodes currently hold
+    void reset()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        key.clear();
+        copies.clear();
+        kernels = 0;
+        host = nullptr;
+        failed = false;
+    }
+};
+
 struct SwPlanInfo {
     bool fast_ok;       // the register kernels apply (sign conditions on the scores)
     bool pack_ok;       // the packed int16x2 kernel applies (scores also small)
@@ -103,6 +142,13 @@ struct gb2_ctx {
     gb2::PipeSet pipe[gb2::kPipeSets];
     gb2::CigarBufs cig;
     cudaEvent_t kdone[gb2::kResidentParts] = {};  // last kernel of each resident part
+    cudaEvent_t ev_join2 = nullptr;  // second executor joined back into the first
+    uint64_t buf_gen = 0;            // bumped whenever a context buffer is reallocated
+    gb2::GraphCache g_sw, g_wfa;     // replay caches of gb2_sw_banded / gb2_wfa_affine
+    // variants installed by gb2_autotune / gb2_tune_set (0 = built-in choice):
+    // SW register kernels of bands 16, 32, 64, 128; the 4-warp WFA kernel
+    int tune_sw[4] = {0, 0, 0, 0};
+    int tune_wfa = 0;
     // statistics
     std::atomic<bool> profiling{false};
     std::mutex prof_mu;

@@ -30,6 +30,7 @@ FLAG_PLAIN = 0x0
 FLAG_BATCHED = 0x1
 FLAG_INT32 = 0x2
 FLAG_GENERIC = 0x4
+FLAG_GRAPH = 0x8  # capture resident calls into a CUDA graph and replay it
 
 
 class SwCfg(ctypes.Structure):
@@ -45,6 +46,18 @@ class SwResult(ctypes.Structure):
 class WfaCfg(ctypes.Structure):
     """gb2_wfa_cfg: WFAConfig (genomics/cpu/align_cpu.mojo:62-68)."""
     _fields_ = [("x", c_i32), ("o", c_i32), ("e", c_i32), ("max_error", c_i32)]
+
+
+GB2_TUNE_SW = 1
+GB2_TUNE_WFA = 2
+GB2_TUNE_MAX = 16
+
+
+class TuneResult(ctypes.Structure):
+    """gb2_tune_result: candidates, their median times and the installed choice."""
+    _fields_ = [("kind", c_i32), ("band_class", c_i32), ("n_candidates", c_i32),
+                ("chosen", c_i32), ("variant", c_i32 * GB2_TUNE_MAX),
+                ("ms", ctypes.c_float * GB2_TUNE_MAX)]
 
 
 class Request(ctypes.Structure):
@@ -109,6 +122,10 @@ SIGNATURES = [
     ("gb2_timer_stop", ctypes.c_int, [vp, P(ctypes.c_float)]),
     ("gb2_stats", ctypes.c_int, [vp, P(ctypes.c_double), P(c_i64), P(c_i64)]),
     ("gb2_stats_reset", ctypes.c_int, [vp]),
+    ("gb2_autotune", ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp, c_i64, ctypes.c_int,
+                                    P(TuneResult)]),
+    ("gb2_tune_set", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("gb2_tune_get", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_int)]),
     ("gb2_set_profiling", ctypes.c_int, [vp, ctypes.c_int]),
     ("gb2_flush_l2", ctypes.c_int, [vp]),
     ("gb2_int_peak", ctypes.c_int, [vp, ctypes.c_int, P(ctypes.c_double)]),

@@ -298,6 +298,39 @@ class GenomicsDevice:
     def stats_reset(self):
         self._check(self.L.gb2_stats_reset(self.ctx))
 
+    # -- autotuner ----------------------------------------------------------------------
+    def autotune(self, kind, q, r, cfg, n_pairs=None, reps=5, bands=None):
+        """gb2_autotune: times every variant of one batched kernel on the resident
+        batches (kind "sw": the register kernel of cfg.band_width's class, inside the
+        whole mixed call when per-pair `bands` are given; "wfa": the WFA kernel),
+        checks they agree, installs the fastest in this context and returns
+        {"band_class", "chosen", "candidates": [(variant, median ms), ...]}."""
+        k = {"sw": _lib.GB2_TUNE_SW, "wfa": _lib.GB2_TUNE_WFA}[kind]
+        c = _sw_cfg(cfg) if k == _lib.GB2_TUNE_SW else _wfa_cfg(cfg)
+        n = min(q.count, r.count) if n_pairs is None else int(n_pairs)
+        b = None
+        if bands is not None:
+            b = np.ascontiguousarray(bands, np.int32)
+            if b.size < n:
+                raise ValueError("bands shorter than n_pairs")
+        res = _lib.TuneResult()
+        self._check(self.L.gb2_autotune(self.ctx, k, q.handle, r.handle, ctypes.byref(c),
+                                        _ptr(b) if b is not None else None, n, int(reps),
+                                        ctypes.byref(res)))
+        return {"band_class": res.band_class, "chosen": res.chosen,
+                "candidates": [(res.variant[i], float(res.ms[i]))
+                               for i in range(res.n_candidates)]}
+
+    def tune_set(self, kind, variant, band_class=0):
+        k = {"sw": _lib.GB2_TUNE_SW, "wfa": _lib.GB2_TUNE_WFA}[kind]
+        self._check(self.L.gb2_tune_set(self.ctx, k, int(band_class), int(variant)))
+
+    def tune_get(self, kind, band_class=0):
+        k = {"sw": _lib.GB2_TUNE_SW, "wfa": _lib.GB2_TUNE_WFA}[kind]
+        v = ctypes.c_int()
+        self._check(self.L.gb2_tune_get(self.ctx, k, int(band_class), ctypes.byref(v)))
+        return v.value
+
     def set_profiling(self, on: bool):
         self._check(self.L.gb2_set_profiling(self.ctx, 1 if on else 0))
 

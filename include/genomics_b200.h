@@ -76,6 +76,10 @@ typedef struct gb2_batch gb2_batch;
 #define GB2_FLAG_BATCHED 0x1   /* length-bucketed device work queue, persistent kernel */
 #define GB2_FLAG_INT32 0x2     /* never take the packed int16 Smith-Waterman path */
 #define GB2_FLAG_GENERIC 0x4   /* force the literal per-pair kernel (testing) */
+#define GB2_FLAG_GRAPH 0x8     /* gb2_sw_banded / gb2_wfa_affine: capture the call's device
+                                  work into a CUDA graph on the second call with the same
+                                  shape (batches, scoring, n_pairs, flags) and replay it on
+                                  later ones; results are those of the eager launches */
 /* Tuning fields (0 = the library's choice): bits 8-15 select a kernel
  * variant; bits 16-23 set how many chunks the *_host entry points split a
  * batch into for their copy/compute pipeline. */
@@ -298,6 +302,40 @@ int gb2_server_wait(gb2_server *srv, uint64_t ticket, int timeout_ms, double *la
 int gb2_server_stats_get(gb2_server *srv, gb2_server_stats *st);
 /* Finish every queued and running request, then stop the thread. */
 int gb2_server_stop(gb2_server *srv);
+
+/* ---- autotuner --------------------------------------------------------------------
+ * The batched kernels come in variants that compute the same results with
+ * different shapes: the int32 Smith-Waterman register kernels split a band row
+ * over G lanes of K columns each (bands 16: G 1/2; 32: G 1/2/4; 64: G 2/4;
+ * 128: G 4/8), and the WFA kernel takes 4, 2 or 1 diagonals per thread per
+ * round with 3-5 resident blocks per SM.  No counterpart in the reference (its
+ * kernels have one fixed shape, genomics/gpu/align_gpu.mojo:60-137).
+ * gb2_autotune runs every candidate of one kernel on a caller's batch (GB2_TUNE_SW:
+ * the register kernel of cfg->band_width's class, forced with GB2_FLAG_INT32;
+ * GB2_TUNE_WFA: the batched WFA kernel), `reps` timed runs each after one
+ * warm-up, checks that every candidate gives the first candidate's results
+ * (GB2_EKERNEL otherwise), and installs the fastest in the context: later calls
+ * whose flags leave the variant field (bits 8-15) at 0 use it.  Tune on the
+ * batch size that will run: a small batch that leaves SMs idle favours more
+ * lanes per pair than a full one.  bands (GB2_TUNE_SW, optional, host): the
+ * per-pair bands of a mixed batch; each candidate of the class then runs inside
+ * the whole mixed call while the other classes keep their installed variants,
+ * so tuning the classes one after another fits the mix.  gb2_tune_set /
+ * gb2_tune_get save and restore the table (variant 0 = the built-in choice). */
+#define GB2_TUNE_SW 1
+#define GB2_TUNE_WFA 2
+#define GB2_TUNE_MAX 16
+typedef struct gb2_tune_result {
+    int32_t kind, band_class;     /* band_class: 16/32/64/128 for GB2_TUNE_SW, 0 for WFA */
+    int32_t n_candidates, chosen; /* chosen: the variant now installed */
+    int32_t variant[GB2_TUNE_MAX];
+    float ms[GB2_TUNE_MAX];       /* median device time of one run per candidate */
+} gb2_tune_result;
+int gb2_autotune(gb2_ctx *ctx, int kind, const gb2_batch *q, const gb2_batch *r,
+                 const void *cfg /* gb2_sw_cfg or gb2_wfa_cfg */, const int32_t *bands,
+                 int64_t n_pairs, int reps, gb2_tune_result *out);
+int gb2_tune_set(gb2_ctx *ctx, int kind, int band_class, int variant);
+int gb2_tune_get(gb2_ctx *ctx, int kind, int band_class, int *variant);
 
 /* ---- pinned host memory -----------------------------------------------------------
  * Page-locked host allocations: SequenceBatch arrays built here reach the
