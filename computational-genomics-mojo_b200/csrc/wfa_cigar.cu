@@ -60,6 +60,8 @@ static int wfa_cigar_run(gb2_ctx *c, SeqView qv, SeqView rv, const int64_t *h_ql
     if ((rc = wfa_begin(c, x)) || (rc = ensure(c, cb.cost, (size_t)n * 4, x.st)) ||
         (rc = ensure(c, cb.hist, (size_t)n * 8, x.st)))
         return rc;
+    const int arena_mib = (int)(((unsigned)flags >> 24) & 0xff);
+    flags &= 0x00ffffff;
     if ((rc = wfa_core(c, x, qv, rv, qmax, rmax, cfg, n, (int32_t *)cb.cost.p,
                        flags | GB2_FLAG_BATCHED, (int64_t *)cb.hist.p)))
         return rc;
@@ -92,7 +94,8 @@ static int wfa_cigar_run(gb2_ctx *c, SeqView qv, SeqView rv, const int64_t *h_ql
                      [&](int32_t a, int32_t b) { return rec[(size_t)a] > rec[(size_t)b]; });
     size_t free_b = 0, total_b = 0;
     GB2_CU(c, cudaMemGetInfo(&free_b, &total_b));
-    int64_t budget = std::min<int64_t>((int64_t)free_b / 2, kCigarArenaCap);
+    int64_t budget = std::min<int64_t>((int64_t)free_b / 2,
+                                       arena_mib ? (int64_t)arena_mib << 20 : kCigarArenaCap);
     if (rec_max >= (1ll << 33))  // header offsets are int32 counts of 4-byte words
         return set_err(c, GB2_ERANGE, "one pair's WFA history needs %lld bytes (limit 8 GiB)",
                        (long long)rec_max);

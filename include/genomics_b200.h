@@ -85,6 +85,9 @@ typedef struct gb2_batch gb2_batch;
  * batch into for their copy/compute pipeline. */
 #define GB2_FLAGS_VARIANT(v) (((v) & 0xff) << 8)
 #define GB2_FLAGS_CHUNKS(n) (((n) & 0xff) << 16)
+/* gb2_wfa_cigar: cap its history arena at n MiB (1-255; 0 = the library's
+   choice), which splits a batch into more groups -- for testing the grouping. */
+#define GB2_FLAGS_ARENA_MIB(n) (((n) & 0xff) << 24)
 
 /* ---- library ----------------------------------------------------------------- */
 
@@ -209,8 +212,8 @@ int gb2_nw_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
  * capacity of `runs`: sum(qlen + rlen) over the pairs always suffices; when
  * the runs do not fit, returns GB2_ERANGE with run_offsets[n_pairs] set to the
  * number needed.  Device history: 5 B per visited wavefront cell + 12 B per
- * score, in groups that fit half the free device memory (at most 16 GiB);
- * GB2_ENOMEM when one pair alone does not fit. */
+ * score, in groups that fit half the free device memory (at most 64 GiB, or
+ * GB2_FLAGS_ARENA_MIB); GB2_ENOMEM when one pair alone does not fit. */
 int gb2_wfa_cigar(gb2_ctx *ctx, const gb2_batch *q, const gb2_batch *r,
                   const gb2_wfa_cfg *cfg, int64_t n_pairs, int32_t *cost,
                   uint32_t *runs, int64_t runs_cap, int64_t *run_offsets, int flags);

@@ -185,3 +185,20 @@ def test_cigar_after_int32_rerun(device):
     assert cost[0] // 2 > 32767 - 31500
     assert _cigar_cost(cig[0], 4, 6, 2) == cost[0]
     assert _cigar_len(cig[0], "=XI") == len(q) and _cigar_len(cig[0], "=XD") == len(r)
+
+
+def test_grouped_arena_matches_one_group(device):
+    """A history arena capped at 2 MiB (GB2_FLAGS_ARENA_MIB) splits these pairs
+    into several groups; costs and CIGARs equal those of one group."""
+    rng = random.Random(77)
+    qs, rs = [], []
+    for _ in range(24):
+        q = "".join(rng.choice("ACGT") for _ in range(rng.randint(500, 2500)))
+        qs.append(q)
+        rs.append(_mutate(rng, q, rng.choice([0.01, 0.03, 0.05])))
+    qb, rb = SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+    cfg = WFAConfig(4, 6, 2, 6000)
+    one = device.wfa_cigar(qb, rb, cfg)
+    grouped = device.wfa_cigar(qb, rb, cfg, flags=2 << 24)
+    assert (one[0] == grouped[0]).all() and list(one[1]) == list(grouped[1])
+    assert (one[0] >= 0).all()
