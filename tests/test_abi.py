@@ -61,6 +61,18 @@ def test_null_arguments_rejected_without_gpu(built_lib):
     assert L.gb2_sync(None) == _lib.GB2_EINVAL
     assert L.gb2_sw_pair(None, None, 0, None, 0, None, None) == _lib.GB2_EINVAL
     assert L.gb2_batch_info(None, None, None) == _lib.GB2_EINVAL
+    res = _lib.TuneResult()
+    assert L.gb2_autotune(None, _lib.GB2_TUNE_SW, None, None, None, None, 1, 1,
+                          ctypes.byref(res)) == _lib.GB2_EINVAL
+    v = ctypes.c_int()
+    assert L.gb2_tune_set(None, _lib.GB2_TUNE_SW, 32, 1) == _lib.GB2_EINVAL
+    assert L.gb2_tune_get(None, _lib.GB2_TUNE_WFA, 0, ctypes.byref(v)) == _lib.GB2_EINVAL
+
+
+def test_tune_result_layout(built_lib):
+    """gb2_tune_result: 4 int32, then GB2_TUNE_MAX int32 variants and floats."""
+    from genomics_b200 import _lib
+    assert ctypes.sizeof(_lib.TuneResult) == 4 * 4 + _lib.GB2_TUNE_MAX * 8
 
 
 def test_sources_compile_for_sm100a():
