@@ -576,7 +576,10 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     int64_t grid = (int64_t)c->sm_count *
                    ((variant & 15) ? (variant & 15) : wfa_blocks_per_sm(variant, bw));
     grid = std::min(grid, std::max<int64_t>(c->sm_count, kWfaScratchCap / (bw * warp_bytes)));
-    grid = std::min(grid, std::max<int64_t>(1, bw == 4 ? (n + 3) / 4 : n));
+    // a plain batch of at most one wave of blocks (a per-call drop-in) runs one
+    // block per pair (below); otherwise no more blocks than the warps need
+    const bool plain_blocks = !(flags & GB2_FLAG_BATCHED) && n <= grid;
+    grid = plain_blocks ? n : std::min(grid, std::max<int64_t>(1, bw == 4 ? (n + 3) / 4 : n));
     int rc;
     if ((rc = ensure(c, x.scratch32, (size_t)(grid * bw * warp_bytes), x.st)) ||
         (rc = ensure(c, x.counters, kCounterBytes, x.st)))
@@ -585,6 +588,12 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     int *const ctr = (int *)x.counters.p;
     PairList longs{nullptr, 0, nullptr, ctr + kCounterStride};
     PairList shorts{nullptr, n, nullptr, ctr};
+    if (plain_blocks) {
+        // every pair, in input order, is aligned by a whole block, so a long pair's
+        // score steps are shared by the block's warps instead of running on one warp
+        longs = PairList{nullptr, n, nullptr, ctr + kCounterStride};
+        shorts = PairList{nullptr, 0, nullptr, ctr};
+    }
     if (flags & GB2_FLAG_BATCHED) {
         const int nb = kLenBuckets;
         // one pair per block for the longest pairs: one wave of blocks of them, or
