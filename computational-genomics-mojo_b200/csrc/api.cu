@@ -336,12 +336,20 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
     const bool force_literal = (flags & GB2_FLAG_GENERIC) != 0;
     const bool batched = (flags & GB2_FLAG_BATCHED) != 0;
     const int variant = (flags >> 8) & 0xff;  // tuning knob (G/K choice), 0 = default
-    // per band class: the caller's variant, else the one installed by the tuner
+    // per band class: the caller's variant, else the one installed by the tuner,
+    // else for a small batch (which leaves most SMs idle) the variant with the
+    // most lanes per pair, which shortens each pair's row loop; else the default
     auto var_of = [&](int cls) -> int {
         if (variant)
             return variant;
         const int slot = cls == 16 ? 0 : cls == 32 ? 1 : cls == 64 ? 2 : cls == 128 ? 3 : -1;
-        return slot >= 0 ? c->tune_sw[slot] : 0;
+        if (slot < 0)
+            return 0;
+        if (c->tune_sw[slot])
+            return c->tune_sw[slot];
+        if (n <= kSwSmallBatch)
+            return cls == 32 ? 2 : 1;  // G = 2, 4, 4, 8 for bands 16, 32, 64, 128
+        return 0;
     };
 
     // literal-kernel scratch (int64 rows), sized for the widest band
