@@ -21,7 +21,8 @@
 // its own and its right neighbour's register and the new value of its left
 // one).  Substitution scores come from per-row equality bits: the reference
 // window's 2-bit codes XOR the replicated query base, folded to one bit per
-// base.  Rows whose cells all lie inside the matrix skip the masking.
+// base.  Rows with no cell left of the reference start skip the masking
+// (cells past the reference end feed no cell inside the matrix).
 // nw_literal_kernel: one thread per pair, int64 rows in global scratch, any
 // band, per-pair bands.
 #include <algorithm>
@@ -100,10 +101,14 @@ nw_band_kernel(SeqView q, SeqView r, SwParams p, int64_t n, int *counter,
                 const uint64_t x = win ^ qrep;
                 eqc[i] = ~(x | (x >> 1)) & 0x5555555555555555ull;
             }
-            // cells j with ri = qi - B + j in [0, rlen)
+            // cells j with ri = qi - B + j in [0, rlen).  Cells past the reference
+            // end (ri >= rlen) need not be NEG: no cell inside the matrix reads
+            // them (diag, up and left of a cell all have ri' <= its ri) and the
+            // score is read inside the matrix, so only rows that reach left of
+            // the reference start take the masked step
             const int lo = max(0, B - qi);
             const int hi = (int)min((int64_t)W, (int64_t)B - qi + rlen);
-            if (lo == 0 && hi == W)
+            if (lo == 0)
                 nw_row<B, false>(H, eqc, lo, hi, p.match, p.mismatch, goe);
             else
                 nw_row<B, true>(H, eqc, lo, hi, p.match, p.mismatch, goe);
