@@ -1052,14 +1052,25 @@ static int pipeline(gb2_ctx *c, const HostSide &hq, const HostSide &hr, const in
             done->store(ci + 1, std::memory_order_release);
         }
     };
-    std::thread tq(scanner, std::cref(hq), &sq, &q_done, 0);
-    std::thread tr(scanner, std::cref(hr), &sr, &r_done, 1);
+    // a small batch (a per-call drop-in among them) is scanned on this thread:
+    // starting two threads would cost more than the scan
+    const bool inline_scan = n <= kInlineScanPairs;
+    std::thread tq, tr;
+    if (inline_scan) {
+        scanner(hq, &sq, &q_done, 0);
+        scanner(hr, &sr, &r_done, 1);
+    } else {
+        tq = std::thread(scanner, std::cref(hq), &sq, &q_done, 0);
+        tr = std::thread(scanner, std::cref(hr), &sr, &r_done, 1);
+    }
     struct Joiner {
         std::thread &a, &b;
         ~Joiner()
         {
-            a.join();
-            b.join();
+            if (a.joinable())
+                a.join();
+            if (b.joinable())
+                b.join();
         }
     } joiner{tq, tr};
     auto issue = [&](int64_t ci) -> int {

@@ -15,6 +15,7 @@ constexpr int kAux = 4;            // auxiliary streams for concurrent band clas
 constexpr int kSwClasses = 7;      // 16, 32, 64, 128, literal, packed 16, packed 32
 constexpr int kLenBuckets = 1024;  // length buckets per class
 constexpr int64_t kSwSmallBatch = 16384;  // SW batches this small take the widest lane split
+constexpr int64_t kInlineScanPairs = 8192;  // host batches this small are scanned inline
 constexpr int64_t kPinChunk = 32ll << 20;
 constexpr int64_t kPackHmax = 511;  // packed kernel: H*128 + column fits 16 bits
 constexpr int64_t kWfaScratchCap = 8ll << 30;  // WFA rings of all warps, bytes
