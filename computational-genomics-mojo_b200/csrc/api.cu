@@ -89,6 +89,18 @@ int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st)
 {
     if (bytes <= b.cap)
         return GB2_OK;
+    if (b.pool) {  // stream-ordered: the old buffer is freed after the work queued on st
+        size_t cap = std::max<size_t>(bytes + bytes / 2, 256);
+        cap = (cap + 255) & ~size_t(255);
+        ++c->buf_gen;
+        if (b.p)
+            CU(c, cudaFreeAsync(b.p, st));
+        b.p = nullptr;
+        b.cap = 0;
+        CU(c, cudaMallocFromPoolAsync(&b.p, cap, b.pool, st));
+        b.cap = cap;
+        return GB2_OK;
+    }
     if (b.p) {
         CU(c, cudaStreamSynchronize(st));
         cudaFree(b.p);

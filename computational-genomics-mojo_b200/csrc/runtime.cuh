@@ -25,6 +25,9 @@ constexpr int64_t kWfaTeamMinLen = 2048;       // shortest WFA pair aligned by a
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    // set: grow by stream-ordered free and allocation from this pool, with
+    // headroom, so growing never synchronises the device (the server's slots)
+    cudaMemPool_t pool = nullptr;
 };
 
 // An executor: one stream (plus auxiliary streams for concurrent band

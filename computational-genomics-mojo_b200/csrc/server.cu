@@ -46,6 +46,10 @@ struct Req {
 struct HostBuf {
     void *p = nullptr;
     size_t cap = 0;
+    // buffers outgrown while the server runs: freed when it stops, because
+    // cudaFreeHost waits for the device, which would stall the groups running
+    // on the other slots
+    std::vector<void *> retired;
 };
 
 int ensure_host(HostBuf &b, size_t bytes)
@@ -53,10 +57,11 @@ int ensure_host(HostBuf &b, size_t bytes)
     if (bytes <= b.cap)
         return GB2_OK;
     if (b.p)
-        cudaFreeHost(b.p);
+        b.retired.push_back(b.p);
     b.p = nullptr;
     b.cap = 0;
-    const size_t cap = std::max<size_t>(bytes + bytes / 4, 1 << 20);
+    // pinning memory is slow: grow with headroom, rarely
+    const size_t cap = std::max<size_t>(2 * bytes, 1 << 20);
     if (cudaMallocHost(&b.p, cap) != cudaSuccess) {
         cudaGetLastError();
         return GB2_ENOMEM;
@@ -139,6 +144,11 @@ struct gb2_server {
     bool stopping = false;
     std::thread th;
     gb2_server_stats st{};
+    // device memory pool of the slots' buffers: they grow by stream-ordered
+    // allocation, so a slot meeting a larger group than before does not stall
+    // the groups running on the other slots (cudaFree would synchronise the
+    // device); freed memory stays in the pool
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -442,12 +452,33 @@ int gb2_server_start(gb2_ctx *c, const gb2_server_cfg *cfg, gb2_server **out)
     gb2_server *s = new gb2_server();
     s->c = c;
     s->cfg = *cfg;
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = c->device;
+        uint64_t keep = UINT64_MAX;
+        if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) !=
+                cudaSuccess) {
+            cudaGetLastError();  // without a pool the slots grow with cudaMalloc
+            if (s->pool)
+                cudaMemPoolDestroy(s->pool);
+            s->pool = nullptr;
+        }
+    }
     for (int i = 0; i < cfg->max_inflight_groups; ++i) {
         auto sl = std::make_unique<Slot>();
+        for (DevBuf *b : {&sl->d_in, &sl->d_out, &sl->x.keys, &sl->x.queue, &sl->x.counts,
+                          &sl->x.seg, &sl->x.counters, &sl->x.scratch64, &sl->x.scratch32,
+                          &sl->x.work, &sl->x.errflag})
+            b->pool = s->pool;
         if (exec_init(sl->x) != GB2_OK) {
             exec_free(sl->x);
             for (auto &o : s->slots)
                 exec_free(o->x);
+            if (s->pool)
+                cudaMemPoolDestroy(s->pool);
             delete s;
             return set_err(c, GB2_ECUDA, "creating a server executor failed");
         }
@@ -610,11 +641,15 @@ int gb2_server_stop(gb2_server *s)
             cudaFree(sl.d_in.p);
         if (sl.d_out.p)
             cudaFree(sl.d_out.p);
-        if (sl.h_in.p)
-            cudaFreeHost(sl.h_in.p);
-        if (sl.h_out.p)
-            cudaFreeHost(sl.h_out.p);
+        for (HostBuf *hb : {&sl.h_in, &sl.h_out}) {
+            if (hb->p)
+                cudaFreeHost(hb->p);
+            for (void *p : hb->retired)
+                cudaFreeHost(p);
+        }
     }
+    if (s->pool)
+        cudaMemPoolDestroy(s->pool);
     for (auto &kv : s->table)
         delete kv.second;
     delete s;
