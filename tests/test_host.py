@@ -132,3 +132,24 @@ def test_max_error_cover():
 def test_sw_cells_convention():
     q, r, b, _ = synth.generate(0, 10)
     assert synth.sw_cells(q, b) == 10 * 150 * 65
+
+
+def test_bench_window_batch_matches_slicing():
+    """bench.py's NW workload: bases [25, 175) of each 200 bp target, repacked."""
+    import sys
+    from conftest import ROOT
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import bench
+    from genomics_b200 import synth
+    _, r, _, _ = synth.generate(1, 300, seed=3)
+    w = bench._window_batch(r, 25, 150, chunk=128)
+    p, _, o, l = r.arrays()
+    pw, _, ow, lw = w.arrays()
+
+    def dec(pp, oo, ll, i):
+        return "".join("ACGT"[(int(pp[oo[i] + k // 32]) >> (62 - 2 * (k % 32))) & 3]
+                       for k in range(int(ll[i])))
+    assert (lw == 150).all()
+    for i in range(0, 300, 37):
+        assert dec(pw, ow, lw, i) == dec(p, o, l, i)[25:175]
