@@ -54,10 +54,13 @@ BAND = 32
 SW_OPS_PER_CELL = 11  # int32 ops per cell of the reference recurrence (align_cpu.mojo:270-296)
 SW_OPS_PER_CELL_PACKED = 5.5  # the same ops on int16x2 lanes: two cells per lane-op
 # dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel per step of this
-# workload: a step runs as 4 launches of 262,144 pairs; one captured launch read 32.02 MB
-# and wrote 0 B (its 3.1 MB of results were still in L2 when it ended), times 4.  From the
-# ncu capture summarised in profiles/sw_pack16_kernel_b32_1M_reads.md
+# workload, from one ncu capture (not measurable inside a timed run): a step runs as 4
+# launches of 262,144 pairs; the captured launch read 32.02 MB and wrote 0 B (its 3.1 MB
+# of results were still in L2 when it ended), times 4.
 SW_PACKED_TRAFFIC_BYTES = 128.1e6
+SW_PACKED_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum of one "
+                            "262,144-pair launch of sw_pack16_kernel<32>, x 4 launches per step "
+                            "(capture of commit 78a5858)")
 
 
 def parse():
@@ -70,6 +73,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the oracle check of every result (outside the timed regions)")
     ap.add_argument("--no-peaks", action="store_true", help="skip the integer-throughput probes")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant knob (tuning)")
     ap.add_argument("--plain", action="store_true", help="plain launch instead of the queue")
@@ -214,6 +219,42 @@ def cpu_sw_gcups(q, r, n_sample: int, threads: int):
     return cells / dt / 1e9, n, dt
 
 
+def cpu_steps(q, r, sample: int, steps: int, warmup: int, threads: int):
+    """The oracle (restatement of align_cpu.mojo) on the first `sample` pairs per step:
+    `warmup` untimed steps on up to 5,000 pairs, then `steps` timed steps.  Returns
+    (GCUPS over the timed steps, total seconds).  The reference arm and the in-run
+    cpu_baseline both use it, so their figures are the same measurement."""
+    for _ in range(warmup):
+        cpu_sw_gcups(q, r, min(sample, 5000), threads)
+    ql = q.arrays()[3]
+    per_step_cells = int((ql[:sample] * (2 * BAND + 1)).sum())
+    total = 0.0
+    for _ in range(steps):
+        total += cpu_sw_gcups(q, r, sample, threads)[2]
+    return per_step_cells * steps / total / 1e9, total
+
+
+def sw_parity(q, r, got, scoring, band, threads, bands=None):
+    """'equal/total' of every pair's (score, query_end, ref_end) against the oracle."""
+    import oracle as O
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    sc, qe, re_ = O.sw_batch(qp, qo, ql, rp, ro, rl, *scoring, band, bands=bands,
+                             threads=threads)
+    ok = (got["score"] == sc) & (got["query_end"] == qe) & (got["ref_end"] == re_)
+    return f"{int(ok.sum())}/{ok.size}"
+
+
+def wfa_parity(q, r, got, cfg, threads):
+    """'equal/total' of every pair's cost against the oracle (live-envelope form)."""
+    import oracle as O
+    qp, _, qo, ql = q.arrays()
+    rp, _, ro, rl = r.arrays()
+    want, _ = O.wfa_batch(qp, qo, ql, rp, ro, rl, cfg.x, cfg.o, cfg.e, cfg.max_error,
+                          envelope=True, threads=threads)
+    return f"{int((want == got).sum())}/{want.size}"
+
+
 def reference_arm(args, dist: Dist):
     """The reference's CPU algorithm, timed on this host's cores."""
     if dist.rank != 0:
@@ -223,17 +264,7 @@ def reference_arm(args, dist: Dist):
     threads = os.cpu_count() or 1
     q, r, _, _ = synth.generate(1, args.pairs)
     sample = min(args.pairs, max(1000, args.cpu_sample // 2))
-    for _ in range(args.warmup):
-        cpu_sw_gcups(q, r, min(sample, 5000), threads)
-    times, cells = [], 0
-    ql = q.arrays()[3]
-    per_step_cells = int((ql[:sample] * (2 * BAND + 1)).sum())
-    for _ in range(args.steps):
-        _, n, dt = cpu_sw_gcups(q, r, sample, threads)
-        times.append(dt)
-        cells += per_step_cells
-    total = sum(times)
-    value = cells / total / 1e9
+    value, total = cpu_steps(q, r, sample, args.steps, args.warmup, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GCUPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -348,20 +379,29 @@ def our_arm(args, dist: Dist):
             mp = json.load(open(mp_path))
         hbm_peak = mp.get("hbm_gbs", 6650.0)
         cpu = None
+        parity = None
         if args.gpus == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            g, n, dt = cpu_sw_gcups(q, r, args.cpu_sample, threads)
+            sample = min(args.pairs, max(1000, args.cpu_sample // 2))
+            csteps = 5
+            g, dt = cpu_steps(q, r, sample, csteps, 3, threads)
             g1, n1, dt1 = cpu_sw_gcups(q, r, max(1000, args.cpu_sample // 5), 1)
             cpu = {"value": round(g, 4), "unit": "GCUPS", "cores": threads, "kind": "port",
-                   "sample": f"first {n} pairs of the workload ({dt:.1f} s)",
+                   "sample": f"first {sample} of the {args.pairs} pairs per step, {csteps} "
+                             f"timed steps after 3 warm-up steps ({dt:.1f} s), as the "
+                             "reference arm",
                    "single_thread": {"value": round(g1, 4), "unit": "GCUPS", "cores": 1,
                                      "sample": f"first {n1} pairs ({dt1:.1f} s), the "
                                                "reference's serial loop"}}
+            if not args.no_parity:
+                # the oracle as the checker: every pair of the timed step's results
+                parity = {"config1_1M_reads": sw_parity(q, r, out, SCORING, BAND, threads)}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "GCUPS",
             "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16x2" if packed else "int32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "pairs_per_gpu": args.pairs, "band": BAND,
                        "query_bp": 150, "target_bp": 200, "scoring": list(SCORING),
                        "path": "batched" if batched else "plain", "variant": args.variant,
@@ -385,12 +425,14 @@ def our_arm(args, dist: Dist):
                                         "max(IADD, IMNMX, 2 x DPX viaddmax) lane-ops/s",
                          "traffic": SW_PACKED_TRAFFIC_BYTES if packed else None,
                          "traffic_unit": "bytes per step, 4 launches (ncu)",
+                         "traffic_source": SW_PACKED_TRAFFIC_SOURCE if packed else None,
                          "hbm": {"achieved": round(alg_bytes / (kernel_ms * 1e-3) / 1e9, 2),
                                  "peak": hbm_peak, "unit": "GB/s",
                                  "frac": round(alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, 5),
                                  "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}},
             "int_peaks_gops": peaks,
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk,
         }
     dq.close()
@@ -423,6 +465,7 @@ def extras(args, dev, peak_ops, hbm_peak):
     with the CPU restatement of the reference beside each (all host threads)."""
     import oracle as O
     from genomics_b200 import AlignConfig, WFAConfig, synth
+    from genomics_b200._lib import FLAG_NAIVE
     O.build()
     threads = os.cpu_count() or 1
     out = {}
@@ -433,6 +476,9 @@ def extras(args, dev, peak_ops, hbm_peak):
     dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
     tb = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=True), 3, 2)
     tp = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=False), 3, 2)
+    tn = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=False,
+                                                flags=FLAG_NAIVE), 2, 1)
+    res_b = np.array(dev.sw_banded(dq, dr, cfg, bands=bands, batched=True))
     m = 3000
     t0 = time.perf_counter()
     qp, _, qo, ql = q.arrays()
@@ -455,12 +501,17 @@ def extras(args, dev, peak_ops, hbm_peak):
         "cells": cells,
         "batched_gcups": round(cells / tb / 1e6, 2), "batched_ms": round(tb, 3),
         "plain_launch_gcups": round(cells / tp / 1e6, 2), "plain_launch_ms": round(tp, 3),
+        "naive_launch_gcups": round(cells / tn / 1e6, 2), "naive_launch_ms": round(tn, 3),
+        "naive_is": "one 128-thread block per pair, input order, no planning (GB2_FLAG_NAIVE)",
         "per_call_gcups": round(call_cells / tcall / 1e9, 3),
         "per_call_pairs_per_s": round(m / tcall, 1),
         "batched_over_per_call": round((cells / tb / 1e6) / (call_cells / tcall / 1e9), 1),
         "cpu_gcups": round(cpu_cells / tcpu / 1e9, 3), "cpu_cores": threads,
         "cpu_sample": f"first {ns} pairs",
     }
+    if not args.no_parity:
+        out["mixed_sw_200k"]["parity"] = sw_parity(q, r, res_b, SCORING, 32, threads,
+                                                   bands=bands)
     # autotuner: the register-kernel shape of each band class, tuned inside the
     # whole mixed batch (one class after another), then the batch timed again
     from genomics_b200 import autotune
@@ -482,7 +533,13 @@ def extras(args, dev, peak_ops, hbm_peak):
     dev.stats_reset()
     tb = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True), 2, 1)
     wcells = dev.stats()["work_units"] // 3
+    wres = np.array(dev.wfa_affine(dq, dr, wcfg, batched=True))
     tp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False), 2, 1)
+    tn = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False,
+                                                 flags=FLAG_NAIVE), 1, 1)
+    # the single-kernel design with rings in global memory (tuning variant 5: five
+    # 4-warp blocks per SM, length-sorted queue) for comparison
+    tg = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True, flags=5 << 8), 1, 1)
     w200 = WFAConfig(4, 6, 2, 200)
     t200 = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, w200, batched=True), 2, 1)
     c200 = dev.wfa_affine(dq, dr, w200, batched=True)
@@ -515,6 +572,10 @@ def extras(args, dev, peak_ops, hbm_peak):
         "wavefront_cells": int(wcells),
         "batched_pairs_per_s": round(n / (tb * 1e-3), 1), "batched_ms": round(tb, 3),
         "plain_launch_pairs_per_s": round(n / (tp * 1e-3), 1), "plain_launch_ms": round(tp, 3),
+        "naive_launch_pairs_per_s": round(n / (tn * 1e-3), 1), "naive_launch_ms": round(tn, 3),
+        "naive_is": "one 4-warp block per pair, input order, rings in global memory, no "
+                    "planning (GB2_FLAG_NAIVE)",
+        "global_ring_kernel_ms": round(tg, 3),
         "per_call_pairs_per_s": round(m / tcall, 1),
         "batched_over_per_call": round((n / (tb * 1e-3)) / (m / tcall), 1),
         "cpu_pairs_per_s": round(ns / tcpu, 2), "cpu_cores": threads,
@@ -532,6 +593,7 @@ def extras(args, dev, peak_ops, hbm_peak):
                              "achieved": round(wbytes / (tb * 1e-3) / 1e9, 2),
                              "peak": hbm_peak, "unit": "GB/s",
                              "frac": round(wbytes / (tb * 1e-3) / 1e9 / hbm_peak, 6)}},
+        "parity": None if args.no_parity else wfa_parity(q, r, wres, wcfg, threads),
         "max_error_200": {"pairs_per_s": round(n / (t200 * 1e-3), 1), "ms": round(t200, 3),
                           "pairs_minus_one": int((c200 < 0).sum()),
                           "note": "the reference's default budget: most long pairs exceed "

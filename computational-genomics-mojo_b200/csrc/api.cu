@@ -42,6 +42,29 @@ int set_err(gb2_ctx *c, int code, const char *fmt, ...)
     return code;
 }
 
+std::atomic<int64_t> g_fail_dev{-1}, g_fail_pin{-1};
+
+int drain_on_error(gb2_ctx *c, int rc)
+{
+    if (rc == GB2_OK || !c)
+        return rc;
+    cudaSetDevice(c->device);
+    auto drain = [](cudaStream_t s) {
+        if (s)
+            cudaStreamSynchronize(s);
+    };
+    for (Exec *x : {&c->x, &c->x2}) {
+        drain(x->st);
+        for (int i = 0; i < kAux; ++i)
+            drain(x->aux[i]);
+    }
+    drain(c->st_copy);
+    drain(c->st_prep);
+    drain(c->st_back);
+    cudaGetLastError();
+    return rc;
+}
+
 int exec_init(Exec &x)
 {
     bool ok = cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking) == cudaSuccess &&
@@ -61,8 +84,9 @@ void exec_free(Exec &x)
     for (int i = 0; i < kAux; ++i)
         if (x.aux[i])
             cudaStreamSynchronize(x.aux[i]);
-    DevBuf *bufs[] = {&x.keys,      &x.queue,     &x.counts, &x.seg,  &x.counters,
-                      &x.scratch64, &x.scratch32, &x.work,   &x.errflag};
+    DevBuf *bufs[] = {&x.keys,      &x.queue,     &x.counts, &x.seg,   &x.counters,
+                      &x.scratch64, &x.scratch32, &x.work,   &x.errflag, &x.tierq,
+                      &x.dumps};
     for (DevBuf *b : bufs)
         if (b->p) {
             cudaFree(b->p);
@@ -97,7 +121,7 @@ int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st)
             CU(c, cudaFreeAsync(b.p, st));
         b.p = nullptr;
         b.cap = 0;
-        CU(c, cudaMallocFromPoolAsync(&b.p, cap, b.pool, st));
+        CU(c, dev_alloc_pool(&b.p, cap, b.pool, st));
         b.cap = cap;
         return GB2_OK;
     }
@@ -110,7 +134,7 @@ int ensure(gb2_ctx *c, DevBuf &b, size_t bytes, cudaStream_t st)
     size_t cap = std::max<size_t>(bytes, 256);
     cap = (cap + 255) & ~size_t(255);
     ++c->buf_gen;  // captured graphs hold buffer addresses: they are stale now
-    CU(c, cudaMalloc(&b.p, cap));
+    CU(c, dev_alloc(&b.p, cap));
     b.cap = cap;
     return GB2_OK;
 }
@@ -205,15 +229,16 @@ __device__ __forceinline__ void count_key(int *counts, int key)
 }
 
 __global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *bands, int32_t band,
-                              int fast_ok, int pack_ok, int32_t match_pos, int32_t *keys,
-                              int *counts)
+                              int fast_ok, int pack_ok, int wide_ok, int32_t match_pos,
+                              int32_t *keys, int *counts)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const int64_t ql = q.lengths[i], rl = r.lengths[i];
     const int32_t b = bands ? bands[i] : band;
-    const int64_t hmax = (int64_t)match_pos * (ql < rl ? ql : rl);  // bound on every H
+    // bound on every H the kernels compute (the row past the query end included)
+    const int64_t hmax = (int64_t)match_pos * ((ql < rl ? ql : rl) + 1);
     int cls = 4;
     if (fast_ok) {
         if (b == 16)
@@ -229,6 +254,8 @@ __global__ void k_classify_sw(int64_t n, SeqView q, SeqView r, const int32_t *ba
         cls = 4;
     if (pack_ok && hmax <= kPackHmax && (cls == 0 || cls == 1))
         cls = cls == 0 ? 5 : 6;
+    else if (wide_ok && hmax <= kWideHmax && cls <= 3)
+        cls = 7 + cls;
     int64_t lb = ql >> 5;
     if (lb > kLenBuckets - 1)
         lb = kLenBuckets - 1;
@@ -371,8 +398,21 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
         return ensure(c, x.scratch64, (size_t)lit_grid * 128 * lit_stride * sizeof(int64_t), x.st);
     };
 
+    if ((flags & GB2_FLAG_NAIVE) && !force_literal && pi.max_band <= kSwNaiveMaxBand) {
+        // the baseline the batched path is measured against: one block per pair,
+        // input order, no planning, per-pair bands read by the kernel
+        cudaEvent_t e0 = profile ? prof_begin(c, x.st) : nullptr;
+        CU(c, launch_sw_naive(qv, rv, p, cfg->band_width, d_bands, std::max(pi.max_band, 0), n,
+                              d_out, x.st));
+        prof_end(c, e0, x.st);
+        c->launches += 1;
+        return GB2_OK;
+    }
     const bool pack = pi.pack_ok && !force_literal && !(flags & GB2_FLAG_INT32);
-    const bool pack_lengths = (int64_t)match_pos * std::min(qmax, rmax) <= kPackHmax;
+    const bool wide = pack && pi.wide_ok;
+    const int64_t hbound = (int64_t)match_pos * (std::min(qmax, rmax) + 1);
+    const bool pack_lengths = hbound <= kPackHmax;
+    const bool wide_lengths = hbound <= kWideHmax;
     // One band for every pair, pairs in input order: no planning kernels.
     // The batched path takes it too when the lengths are narrow (nothing to
     // sort), with a dynamic pair counter.
@@ -380,6 +420,8 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
         int cls = (pi.fast_ok && lengths_ok && !force_literal) ? classify_band(cfg->band_width) : 0;
         if ((cls == 16 || cls == 32) && pack && pack_lengths)
             cls |= kPack16;
+        else if (cls > 0 && wide && wide_lengths)
+            cls |= kPackWide;
         PairList pl{nullptr, n, nullptr, nullptr};
         int grid = 0;  // one pair per thread, pairs in input order
         if (batched && cls > 0) {  // persistent blocks taking pairs from a counter
@@ -420,8 +462,8 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
     const int fast = (pi.fast_ok && !force_literal) ? 1 : 0;
     const int blocks = (int)((n + 255) / 256);
     k_classify_sw<<<blocks, 256, 0, x.st>>>(n, qv, rv, d_bands, cfg->band_width, fast,
-                                             pack ? 1 : 0, match_pos, (int32_t *)x.keys.p,
-                                             (int *)x.counts.p);
+                                             pack ? 1 : 0, wide ? 1 : 0, match_pos,
+                                             (int32_t *)x.keys.p, (int *)x.counts.p);
     k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, kLenBuckets, (int64_t *)x.seg.p);
     k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
                                          (int32_t *)x.queue.p);
@@ -430,27 +472,39 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
 
     // One persistent launch per class that can hold pairs; classes run
     // concurrently on the auxiliary streams.
-    static const int cls_band[kSwClasses] = {16, 32, 64, 128, 0, 16 | kPack16, 32 | kPack16};
+    static const int cls_band[kSwClasses] = {16, 32, 64, 128, 0, 16 | kPack16, 32 | kPack16,
+                                             16 | kPackWide, 32 | kPackWide, 64 | kPackWide,
+                                             128 | kPackWide};
     static_assert(kSwClasses * kCounterStride * 4 <= (int)kCounterBytes, "counter space");
-    bool need[kSwClasses] = {false, false, false, false, true, false, false};
+    bool need[kSwClasses] = {false, false, false, false, true, false,
+                             false, false, false, false, false};
     if (pi.uniform_band) {
         const int cb = classify_band(cfg->band_width);
         for (int k = 0; k < 4; ++k)
             need[k] = fast && cls_band[k] == cb;
         need[5] = pack && cb == 16;
         need[6] = pack && cb == 32;
+        for (int k = 0; k < 4; ++k)
+            need[7 + k] = wide && cls_band[k] == cb;
         // when the batch's longest sequences qualify, every pair lands in one
         // class: skip the launches that would find nothing
         if (need[5] || need[6]) {
             need[0] = need[0] && !pack_lengths;
             need[1] = need[1] && !pack_lengths;
+            for (int k = 7; k < 9; ++k)
+                need[k] = need[k] && !pack_lengths;
         }
+        for (int k = 0; k < 4; ++k)
+            if (need[7 + k])
+                need[k] = need[k] && !wide_lengths;
         need[4] = !(fast && cb > 0 && lengths_ok);
     } else {
         for (int k = 0; k < 4; ++k)
             need[k] = fast && cls_band[k] <= std::max<int32_t>(pi.max_band, 0);
         need[5] = pack && pi.max_band >= 16;
         need[6] = pack && pi.max_band >= 32;
+        for (int k = 0; k < 4; ++k)
+            need[7 + k] = wide && (cls_band[k] & 0xff) <= std::max<int32_t>(pi.max_band, 0);
     }
     if (need[4] && (rc = ensure_lit()))
         return rc;
@@ -511,6 +565,7 @@ int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t
     pi.pack_ok = pi.fast_ok && cfg->mismatch >= goe && cfg->match_score >= cfg->mismatch &&
                  cfg->match_score <= 255 && -goe <= 255 && -cfg->gap_extend <= 255 &&
                  cfg->match_score - cfg->mismatch <= 255;
+    pi.wide_ok = pi.pack_ok && cfg->match_score <= 127;
     pi.max_band = maxb;
     pi.uniform_band = bands == nullptr;
     return GB2_OK;
@@ -571,6 +626,116 @@ static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
     return n <= kWfaWideMaxPairs && std::max(qmax, rmax) >= kWfaWideTeamLen ? kWfaWideWarps : 4;
 }
 
+// Tiered WFA (wfa_tiers.cu): every pair starts on the smallest team whose
+// launch still fills the GPU -- one warp (S) for large batches, four warps (M)
+// for up to 16 pairs per SM, sixteen (L) for up to two per SM, so a single long
+// pair (the per-call drop-in) gets a whole SM -- and moves up a tier when its
+// wavefront outgrows the window; pairs that outgrow L or need int32 rows
+// finish in G.  One launch per tier from the first, in order on x.st; the
+// launches after the first take their pair count from the device.  With
+// GB2_FLAG_BATCHED the first tier's queue is ordered longest first.
+static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
+                     const WfaParams &p, int64_t n, int32_t *d_out, int flags)
+{
+    const WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
+    const int64_t sms = c->sm_count;
+    int first = n <= 2 * sms ? 2 : (n <= 16 * sms ? 1 : 0);
+    while (first < 3 && !pl.usable[first])
+        ++first;
+    auto next_of = [&](int t) {
+        for (int u = t + 1; u < 3; ++u)
+            if (pl.usable[u])
+                return u;
+        return -1;
+    };
+    // dump records of the transitions out of the first two tiers
+    int64_t dcap[3] = {0, 0, 0}, doff[3] = {0, 0, 0}, dbytes = 0;
+    for (int t = first; t < 3; ++t) {
+        if (!pl.usable[t] || next_of(t) < 0)
+            continue;
+        dcap[t] = std::min<int64_t>(n, kTierDumpCap / pl.dump_stride[t]);
+        doff[t] = dbytes;
+        dbytes += dcap[t] * pl.dump_stride[t];
+    }
+    int rc;
+    if ((rc = ensure(c, x.tierq, (size_t)n * 24, x.st)) ||
+        (rc = ensure(c, x.dumps, (size_t)std::max<int64_t>(dbytes, 256), x.st)) ||
+        (rc = ensure(c, x.scratch32, (size_t)(sms * pl.gring_block_bytes), x.st)) ||
+        (rc = ensure(c, x.counters, kCounterBytes, x.st)))
+        return rc;
+    CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
+    int *const ctr = (int *)x.counters.p;
+    int *const in_ctr = ctr;                         // + 32 * tier
+    int *const q_n = ctr + 4 * kCounterStride;       // + 32 * (tier - 1): pairs queued for M, L, G
+    int *const d_ctr = ctr + 7 * kCounterStride;     // + 32 * tier: records claimed
+    int2 *const tq = (int2 *)x.tierq.p;              // + n * (tier - 1)
+    uint8_t *const dumps = (uint8_t *)x.dumps.p;
+    const int32_t *list = nullptr;
+    const int64_t *seg = nullptr;
+    if (flags & GB2_FLAG_BATCHED) {
+        const int nb = kLenBuckets;
+        if ((rc = ensure(c, x.keys, (size_t)n * 4, x.st)) ||
+            (rc = ensure(c, x.queue, (size_t)n * 4, x.st)) ||
+            (rc = ensure(c, x.counts, (size_t)nb * 4, x.st)) ||
+            (rc = ensure(c, x.seg, 64, x.st)))
+            return rc;
+        CU(c, cudaMemsetAsync(x.counts.p, 0, (size_t)nb * 4, x.st));
+        const int blocks = (int)((n + 255) / 256);
+        k_classify_wfa<<<blocks, 256, 0, x.st>>>(n, qv, rv, (int32_t *)x.keys.p,
+                                                  (int *)x.counts.p);
+        k_scan<<<1, 1024, 0, x.st>>>((int *)x.counts.p, nb, nb, (int64_t *)x.seg.p);
+        k_scatter<<<blocks, 256, 0, x.st>>>(n, (const int32_t *)x.keys.p, (int *)x.counts.p,
+                                             (int32_t *)x.queue.p);
+        CU(c, cudaGetLastError());
+        c->launches += 3;
+        list = (const int32_t *)x.queue.p;
+        seg = (const int64_t *)x.seg.p;
+    }
+    static const int teams_per_block[4] = {16, 4, 1, 1};
+    int prev = -1;  // the tier launched before t: its suspended pairs are t's entries
+    for (int t = first; t < 4; ++t) {
+        if (t < 3 && !pl.usable[t])
+            continue;
+        WfaTierIo io{};
+        io.ctr = in_ctr + kCounterStride * t;
+        if (t == first) {
+            io.list = list;
+            io.seg = seg;
+            io.n = n;
+        } else {
+            io.ents = tq + n * (t - 1);
+            io.n_dev = q_n + kCounterStride * (t - 1);
+            if (t < 3 && prev >= 0 && dcap[prev] > 0) {  // G entries always start over
+                io.dumps_in = dumps + doff[prev];
+                io.dump_in_stride = pl.dump_stride[prev];
+            }
+        }
+        const int nt = t < 3 ? next_of(t) : -1;
+        if (nt >= 0) {
+            io.next = tq + n * (nt - 1);
+            io.next_n = q_n + kCounterStride * (nt - 1);
+            io.dumps_out = dumps + doff[t];
+            io.dump_out_stride = pl.dump_stride[t];
+            io.dump_out_cap = dcap[t];
+            io.dump_out_ctr = d_ctr + kCounterStride * t;
+        }
+        if (t < 3) {
+            io.restart = tq + n * 2;
+            io.restart_n = q_n + kCounterStride * 2;
+        }
+        io.gring = (int32_t *)x.scratch32.p;
+        const int64_t per = teams_per_block[t];
+        const int grid = (int)(t == first ? std::min<int64_t>(sms, (n + per - 1) / per) : sms);
+        cudaEvent_t e0 = prof_begin(c, x.st);
+        CU(c, launch_wfa_tier(pl, t, grid, qv, rv, p, io, d_out, (int64_t *)x.work.p,
+                              (int *)x.errflag.p, x.st));
+        prof_end(c, e0, x.st);
+        c->launches += 1;
+        prev = t;
+    }
+    return GB2_OK;
+}
+
 int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
              const gb2_wfa_cfg *cfg, int64_t n, int32_t *d_out, int flags, int64_t *d_hist)
 {
@@ -579,6 +744,10 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     if (qmax >= (1ll << 30) || rmax >= (1ll << 30))
         return set_err(c, GB2_ERANGE, "sequence longer than 2^30");
     const WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
+    // the tiered kernels, unless the call asks for the naive baseline, a tuning
+    // variant of the single-kernel design below, or the CIGAR pass's history sizes
+    if (!(flags & GB2_FLAG_NAIVE) && ((flags >> 8) & 0xff) == 0 && !d_hist)
+        return wfa_tiers(c, x, qv, rv, qmax, rmax, p, n, d_out, flags);
     const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
     const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
     const int nslot = hm + 2 * hie;
@@ -599,7 +768,11 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     // a plain batch of at most one wave of blocks (a per-call drop-in) runs one
     // block per pair (below); otherwise no more blocks than the warps need
     const bool plain_blocks = !(flags & GB2_FLAG_BATCHED) && n <= grid;
-    grid = plain_blocks ? n : std::min(grid, std::max<int64_t>(1, bw == 4 ? (n + 3) / 4 : n));
+    // the naive baseline: every pair, in input order, by a whole block (blocks
+    // take the next pair when done, so the rings stay one region per block)
+    const bool naive = (flags & GB2_FLAG_NAIVE) != 0;
+    grid = plain_blocks ? n
+                        : std::min(grid, std::max<int64_t>(1, (bw == 4 && !naive) ? (n + 3) / 4 : n));
     int rc;
     if ((rc = ensure(c, x.scratch32, (size_t)(grid * bw * warp_bytes), x.st)) ||
         (rc = ensure(c, x.counters, kCounterBytes, x.st)))
@@ -608,13 +781,13 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     int *const ctr = (int *)x.counters.p;
     PairList longs{nullptr, 0, nullptr, ctr + kCounterStride};
     PairList shorts{nullptr, n, nullptr, ctr};
-    if (plain_blocks) {
+    if (plain_blocks || naive) {
         // every pair, in input order, is aligned by a whole block, so a long pair's
         // score steps are shared by the block's warps instead of running on one warp
         longs = PairList{nullptr, n, nullptr, ctr + kCounterStride};
         shorts = PairList{nullptr, 0, nullptr, ctr};
     }
-    if (flags & GB2_FLAG_BATCHED) {
+    if ((flags & GB2_FLAG_BATCHED) && !naive) {
         const int nb = kLenBuckets;
         // one pair per block for the longest pairs: one wave of blocks of them, or
         // with the wide kernel every pair of at least kWfaWideTeamLen bases
@@ -796,7 +969,7 @@ static int pin_out(gb2_ctx *c, size_t bytes)
         cudaFreeHost(c->pin_out);
     c->pin_out = nullptr;
     c->pin_out_cap = 0;
-    CU(c, cudaMallocHost(&c->pin_out, bytes));
+    CU(c, pinned_alloc(&c->pin_out, bytes));
     c->pin_out_cap = bytes;
     return GB2_OK;
 }
@@ -1013,7 +1186,7 @@ static int ensure_len32(gb2_ctx *c, size_t bytes)
     c->pin_len32 = nullptr;
     c->pin_len32_cap = 0;
     const size_t cap = std::max<size_t>(bytes + bytes / 4, 1 << 16);
-    CU(c, cudaMallocHost(&c->pin_len32, cap));
+    CU(c, pinned_alloc(&c->pin_len32, cap));
     c->pin_len32_cap = cap;
     return GB2_OK;
 }
@@ -1190,6 +1363,14 @@ extern "C" {
 
 int gb2_version(void) { return GB2_VERSION_NUM; }
 
+int gb2_debug_fail_alloc(int kind, int64_t nth)
+{
+    if (kind != GB2_ALLOC_DEVICE && kind != GB2_ALLOC_PINNED)
+        return GB2_EINVAL;
+    (kind == GB2_ALLOC_DEVICE ? g_fail_dev : g_fail_pin).store(nth < 0 ? -1 : nth);
+    return GB2_OK;
+}
+
 const char *gb2_strerror(int status)
 {
     switch (status) {
@@ -1203,6 +1384,7 @@ const char *gb2_strerror(int status)
     case GB2_ESTATE: return "wrong state";
     case GB2_EKERNEL: return "kernel reported an error";
     case GB2_ESCRATCH: return "request exceeds the fixed no-allocation scratch";
+    case GB2_ECANCELED: return "cancelled";
     default: return "unknown status";
     }
 }
@@ -1235,7 +1417,7 @@ int gb2_create(int device, gb2_ctx **out)
               cudaStreamCreateWithFlags(&c->st_back, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
     for (int i = 0; ok && i < 2; ++i) {
-        ok = cudaMallocHost(&c->pin[i], (size_t)kPinChunk) == cudaSuccess &&
+        ok = pinned_alloc(&c->pin[i], (size_t)kPinChunk) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming) == cudaSuccess;
         if (ok)
             cudaEventRecord(c->pin_ev[i], c->x.st);
@@ -1337,7 +1519,7 @@ const char *gb2_last_error(gb2_ctx *c)
     return c->last_error.c_str();
 }
 
-int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const uint64_t *nmask,
+static int gb2_batch_upload_impl(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const uint64_t *nmask,
                      const int64_t *offsets, const int64_t *lengths, int64_t count,
                      gb2_batch **out)
 {
@@ -1365,13 +1547,13 @@ int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const 
     b->min_len = minlen;
     const size_t wb = (size_t)std::max<int64_t>(n_words, 1) * 8;
     const size_t sb = (size_t)std::max<int64_t>(count, 1) * 8;
-    cudaError_t e = cudaMalloc(&b->d_packed, wb);
+    cudaError_t e = dev_alloc(&b->d_packed, wb);
     if (e == cudaSuccess && nmask)
-        e = cudaMalloc(&b->d_nmask, wb);
+        e = dev_alloc(&b->d_nmask, wb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&b->d_offsets, sb);
+        e = dev_alloc(&b->d_offsets, sb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&b->d_lengths, sb);
+        e = dev_alloc(&b->d_lengths, sb);
     auto release = [&]() {
         cudaFree(b->d_packed);
         cudaFree(b->d_nmask);
@@ -1406,6 +1588,13 @@ int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const 
     return GB2_OK;
 }
 
+int gb2_batch_upload(gb2_ctx *c, const uint64_t *packed, int64_t n_words, const uint64_t *nmask,
+                     const int64_t *offsets, const int64_t *lengths, int64_t count,
+                     gb2_batch **out)
+{
+    return drain_on_error(c, gb2_batch_upload_impl(c, packed, n_words, nmask, offsets, lengths, count, out));
+}
+
 int gb2_batch_free(gb2_ctx *c, gb2_batch *b)
 {
     if (!c || !b || b->owner != c)
@@ -1432,7 +1621,7 @@ int gb2_batch_info(const gb2_batch *b, int64_t *count, int64_t *n_words)
     return GB2_OK;
 }
 
-int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
+static int gb2_sw_banded_impl(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
                   const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
 {
     if (!c || !q || !r)
@@ -1537,7 +1726,13 @@ int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
     return GB2_OK;
 }
 
-int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
+int gb2_sw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
+                  const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
+{
+    return drain_on_error(c, gb2_sw_banded_impl(c, q, r, cfg, bands, n, out, flags));
+}
+
+static int gb2_sw_banded_host_impl(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
                        const int64_t *q_lengths, const uint64_t *r_packed,
                        const int64_t *r_offsets, const int64_t *r_lengths, const gb2_sw_cfg *cfg,
                        const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
@@ -1571,7 +1766,15 @@ int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_of
                     });
 }
 
-int gb2_sw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+int gb2_sw_banded_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
+                       const int64_t *q_lengths, const uint64_t *r_packed,
+                       const int64_t *r_offsets, const int64_t *r_lengths, const gb2_sw_cfg *cfg,
+                       const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
+{
+    return drain_on_error(c, gb2_sw_banded_host_impl(c, q_packed, q_offsets, q_lengths, r_packed, r_offsets, r_lengths, cfg, bands, n, out, flags));
+}
+
+static int gb2_sw_pair_impl(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
                 int64_t rlen, const gb2_sw_cfg *cfg, gb2_sw_result *out)
 {
     if (!c)
@@ -1584,7 +1787,13 @@ int gb2_sw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_
                               &rlen, cfg, nullptr, 1, out, GB2_FLAG_PLAIN);
 }
 
-int gb2_wfa_affine(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
+int gb2_sw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+                int64_t rlen, const gb2_sw_cfg *cfg, gb2_sw_result *out)
+{
+    return drain_on_error(c, gb2_sw_pair_impl(c, q_words, qlen, r_words, rlen, cfg, out));
+}
+
+static int gb2_wfa_affine_impl(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
                    int64_t n, int32_t *out, int flags)
 {
     if (!c || !q || !r)
@@ -1621,7 +1830,13 @@ int gb2_wfa_affine(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2
     return d2h_results(c, out, c->out_wfa.p, (size_t)n * 4);
 }
 
-int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
+int gb2_wfa_affine(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
+                   int64_t n, int32_t *out, int flags)
+{
+    return drain_on_error(c, gb2_wfa_affine_impl(c, q, r, cfg, n, out, flags));
+}
+
+static int gb2_wfa_affine_host_impl(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
                         const int64_t *q_lengths, const uint64_t *r_packed,
                         const int64_t *r_offsets, const int64_t *r_lengths,
                         const gb2_wfa_cfg *cfg, int64_t n, int32_t *out, int flags)
@@ -1653,7 +1868,15 @@ int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_o
     return r1 ? r1 : r2;
 }
 
-int gb2_wfa_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+int gb2_wfa_affine_host(gb2_ctx *c, const uint64_t *q_packed, const int64_t *q_offsets,
+                        const int64_t *q_lengths, const uint64_t *r_packed,
+                        const int64_t *r_offsets, const int64_t *r_lengths,
+                        const gb2_wfa_cfg *cfg, int64_t n, int32_t *out, int flags)
+{
+    return drain_on_error(c, gb2_wfa_affine_host_impl(c, q_packed, q_offsets, q_lengths, r_packed, r_offsets, r_lengths, cfg, n, out, flags));
+}
+
+static int gb2_wfa_pair_impl(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
                  int64_t rlen, const gb2_wfa_cfg *cfg, int32_t *out)
 {
     if (!c)
@@ -1666,12 +1889,18 @@ int gb2_wfa_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64
                                &rlen, cfg, 1, out, GB2_FLAG_PLAIN);
 }
 
+int gb2_wfa_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+                 int64_t rlen, const gb2_wfa_cfg *cfg, int32_t *out)
+{
+    return drain_on_error(c, gb2_wfa_pair_impl(c, q_words, qlen, r_words, rlen, cfg, out));
+}
+
 int gb2_host_alloc(int64_t bytes, void **out)
 {
     if (!out || bytes < 0)
         return GB2_EINVAL;
     *out = nullptr;
-    if (cudaMallocHost(out, (size_t)std::max<int64_t>(bytes, 8)) != cudaSuccess) {
+    if (pinned_alloc(out, (size_t)std::max<int64_t>(bytes, 8)) != cudaSuccess) {
         cudaGetLastError();
         *out = nullptr;
         return GB2_ENOMEM;

@@ -67,8 +67,11 @@ struct SwParams {
     int32_t match, mismatch, go, ge;
 };
 
-// band_class flag selecting the packed int16x2 kernel (bands 16 and 32).
+// band_class flags selecting the packed int16x2 kernel: kPack16 with keys for
+// scores up to 511 (bands 16 and 32), kPackWide with group keys for scores up
+// to 4094 (bands 16, 32, 64, 128).
 constexpr int kPack16 = 0x100;
+constexpr int kPackWide = 0x200;
 
 // Smith-Waterman launch over a list of pair indices (queue == nullptr means
 // pairs [0, n)).  `bands` (device, may be nullptr) overrides `band`.
@@ -77,6 +80,12 @@ constexpr int kPack16 = 0x100;
 cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParams p,
                       int32_t band, const int32_t *bands, PairList pl, gb2_sw_result *out,
                       int64_t *scratch, int64_t scratch_stride, int grid, cudaStream_t st);
+
+// The naive baseline: one 128-thread block per pair, pairs in input order
+// (grid = n), int32 band rows in shared memory (2 * (2 * max_band + 1) ints).
+constexpr int32_t kSwNaiveMaxBand = 4096;
+cudaError_t launch_sw_naive(SeqView q, SeqView r, SwParams p, int32_t band, const int32_t *bands,
+                            int32_t max_band, int64_t n, gb2_sw_result *out, cudaStream_t st);
 
 // Pairs per 128-thread block, and resident blocks per SM, of a kernel variant.
 int sw_pairs_per_block(int band_class, int variant);
@@ -99,6 +108,49 @@ cudaError_t launch_wfa(int variant, int block_warps, SeqView q, SeqView r, WfaPa
                        PairList longs, PairList shorts, int32_t *out, int32_t *scratch,
                        int64_t slot_width, int grid, int *err_flag, int64_t *work, int64_t *hist,
                        cudaStream_t st);
+
+// Tiered WFA (wfa_tiers.cu): tier 0 (S) one warp per pair, 1 (M) four warps,
+// 2 (L) sixteen warps, rings of W int16 per slot in shared memory; tier 3 (G)
+// sixteen warps, int32 rings in global memory covering every diagonal.
+struct WfaTierPlan {
+    int nslot;
+    int32_t W[4], H[4];        // window per slot row; element of diagonal 0
+    int32_t seq_cap[4];        // 16-base window entries of a sequence copy
+    int64_t team_bytes[4];     // shared bytes per team
+    int64_t ring_bytes[4];     // of them, the ring
+    int64_t dump_stride[3];    // bytes of a suspended pair's record, per source tier
+    bool usable[4];            // the window holds at least 64 diagonals
+    int64_t gring_block_bytes; // G tier ring region of one block
+};
+WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax);
+
+// Inputs and outputs of one tier launch.  Input: list (int32 pair indices,
+// nullptr = 0..n-1) or ents ({pair, dump record or -1}); n, or *n_dev when set,
+// or seg[0..1] = [start, end) of list; ctr hands items out (zeroed).  Output:
+// suspended pairs go to next (count next_n) with their record in dumps_out
+// (dump_out_ctr records claimed of dump_out_cap); pairs that must restart go to
+// restart (count restart_n).
+struct WfaTierIo {
+    const int32_t *list;
+    const int2 *ents;
+    int64_t n;
+    const int *n_dev;
+    const int64_t *seg;
+    int *ctr;
+    const uint8_t *dumps_in;
+    int64_t dump_in_stride;
+    int2 *next;
+    int *next_n;
+    uint8_t *dumps_out;
+    int64_t dump_out_stride, dump_out_cap;
+    int *dump_out_ctr;
+    int2 *restart;
+    int *restart_n;
+    int32_t *gring;  // G tier: grid regions of gring_block_bytes
+};
+cudaError_t launch_wfa_tier(const WfaTierPlan &pl, int tier, int grid, SeqView q, SeqView r,
+                            WfaParams p, const WfaTierIo &io, int32_t *out, int64_t *work,
+                            int *err_flag, cudaStream_t st);
 
 // WFA history record of one pair (the CIGAR traceback's input), at a 16-byte
 // aligned offset of an arena: int32 header[3 * S] (per visited score index:

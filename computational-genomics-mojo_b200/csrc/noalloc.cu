@@ -118,8 +118,10 @@ extern "C" int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
     const int64_t want = (n_pairs + 3) / 4;
     if (blocks > want)
         blocks = want;
-    if (blocks > (int64_t)sms * 4)
-        blocks = (int64_t)sms * 4;
+    // as many blocks as stay resident (the allocating path's grid), at most
+    const int64_t resident = (int64_t)sms * gb2::wfa_blocks_per_sm(0, 4);
+    if (blocks > resident)
+        blocks = resident;
 
     cudaStream_t st = (cudaStream_t)stream;
     unsigned char *const hdr = (unsigned char *)base;

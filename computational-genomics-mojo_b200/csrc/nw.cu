@@ -257,7 +257,7 @@ static int nw_core(gb2_ctx *c, SeqView qv, SeqView rv, int64_t qmax, int64_t rma
 
 extern "C" {
 
-int gb2_nw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
+static int gb2_nw_banded_impl(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
                   const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
 {
     if (!c || !q || !r)
@@ -286,7 +286,13 @@ int gb2_nw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
     return GB2_OK;
 }
 
-int gb2_nw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+int gb2_nw_banded(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_sw_cfg *cfg,
+                  const int32_t *bands, int64_t n, gb2_sw_result *out, int flags)
+{
+    return drain_on_error(c, gb2_nw_banded_impl(c, q, r, cfg, bands, n, out, flags));
+}
+
+static int gb2_nw_pair_impl(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
                 int64_t rlen, const gb2_sw_cfg *cfg, gb2_sw_result *out)
 {
     if (!c || !out || qlen < 0 || rlen < 0 || (qlen > 0 && !q_words) || (rlen > 0 && !r_words))
@@ -305,6 +311,12 @@ int gb2_nw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_
     gb2_batch_free(c, qb);
     gb2_batch_free(c, rb);
     return rc;
+}
+
+int gb2_nw_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen, const uint64_t *r_words,
+                int64_t rlen, const gb2_sw_cfg *cfg, gb2_sw_result *out)
+{
+    return drain_on_error(c, gb2_nw_pair_impl(c, q_words, qlen, r_words, rlen, cfg, out));
 }
 
 }  // extern "C"

@@ -64,7 +64,7 @@ k_pack_ascii(const uint8_t *__restrict__ ascii, const int64_t *__restrict__ star
 
 extern "C" {
 
-int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
+static int gb2_batch_from_ascii_impl(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
                          const int64_t *starts, const int64_t *lengths, int64_t count,
                          gb2_batch **out)
 {
@@ -97,17 +97,17 @@ int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
     int64_t *d_starts = nullptr;
     const size_t wb = (size_t)std::max<int64_t>(words, 1) * 8;
     const size_t sb = (size_t)std::max<int64_t>(count, 1) * 8;
-    cudaError_t e = cudaMalloc(&b->d_packed, wb);
+    cudaError_t e = dev_alloc(&b->d_packed, wb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&b->d_nmask, wb);
+        e = dev_alloc(&b->d_nmask, wb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&b->d_offsets, sb);
+        e = dev_alloc(&b->d_offsets, sb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&b->d_lengths, sb);
+        e = dev_alloc(&b->d_lengths, sb);
     if (e == cudaSuccess)
-        e = cudaMalloc(&d_ascii, (size_t)std::max<int64_t>(ascii_bytes, 1));
+        e = dev_alloc(&d_ascii, (size_t)std::max<int64_t>(ascii_bytes, 1));
     if (e == cudaSuccess)
-        e = cudaMalloc(&d_starts, sb);
+        e = dev_alloc(&d_starts, sb);
     int rc = GB2_OK;
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -149,6 +149,13 @@ int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
     }
     *out = b;
     return GB2_OK;
+}
+
+int gb2_batch_from_ascii(gb2_ctx *c, const uint8_t *ascii, int64_t ascii_bytes,
+                         const int64_t *starts, const int64_t *lengths, int64_t count,
+                         gb2_batch **out)
+{
+    return drain_on_error(c, gb2_batch_from_ascii_impl(c, ascii, ascii_bytes, starts, lengths, count, out));
 }
 
 int gb2_batch_download(gb2_ctx *c, const gb2_batch *b, uint64_t *packed, uint64_t *nmask,

@@ -12,14 +12,22 @@
 namespace gb2 {
 
 constexpr int kAux = 4;            // auxiliary streams for concurrent band classes
-constexpr int kSwClasses = 7;      // 16, 32, 64, 128, literal, packed 16, packed 32
+// 16, 32, 64, 128 (int32 registers), literal, packed 16, packed 32 (narrow keys),
+// packed 16, 32, 64, 128 (wide keys)
+constexpr int kSwClasses = 11;
 constexpr int kLenBuckets = 1024;  // length buckets per class
 constexpr int64_t kSwSmallBatch = 16384;  // SW batches this small take the widest lane split
 constexpr int64_t kInlineScanPairs = 8192;  // host batches this small are scanned inline
 constexpr int64_t kPinChunk = 32ll << 20;
-constexpr int64_t kPackHmax = 511;  // packed kernel: H*128 + column fits 16 bits
+// Packed int16x2 kernels: every cell they compute (the in-matrix ones, and the
+// row past the query end, which adds at most `match`) stays below these, checked
+// as match * (min(qlen, rlen) + 1): H*128 + column fits 16 bits (narrow keys),
+// H*8 + 7 fits a signed 16-bit half (wide keys).
+constexpr int64_t kPackHmax = 511;
+constexpr int64_t kWideHmax = 4094;
 constexpr int64_t kWfaScratchCap = 8ll << 30;  // WFA rings of all warps, bytes
 constexpr int64_t kWfaTeamMinLen = 2048;       // shortest WFA pair aligned by a whole block
+constexpr int64_t kTierDumpCap = 1ll << 30;    // bytes of suspended-pair records per transition
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -38,6 +46,7 @@ struct Exec {
     cudaStream_t aux[kAux] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
     DevBuf keys, queue, counts, seg, counters, scratch64, scratch32, work, errflag;
+    DevBuf tierq, dumps;  // tiered WFA: the M/L/G queues and the suspended pairs' records
 };
 
 // Device buffers of the WFA CIGAR entry point (grow-only, per context).
@@ -102,6 +111,7 @@ struct GraphCache {
 struct SwPlanInfo {
     bool fast_ok;       // the register kernels apply (sign conditions on the scores)
     bool pack_ok;       // the packed int16x2 kernel applies (scores also small)
+    bool wide_ok;       // ... and with its wide keys (match <= 127)
     int32_t max_band;
     bool uniform_band;  // no per-pair bands
     // set by the caller when every pair's lengths lie in a narrow range: a
@@ -170,6 +180,42 @@ namespace gb2 {
 
 int set_err(gb2_ctx *c, int code, const char *fmt, ...);
 
+// Allocation fault injection (gb2_debug_fail_alloc): a countdown per kind;
+// the allocation that finds it at zero fails as out of memory, and the
+// countdown turns off (-1).  Every device and pinned allocation of the
+// library goes through these helpers.
+extern std::atomic<int64_t> g_fail_dev, g_fail_pin;
+inline bool injected_failure(std::atomic<int64_t> &cd)
+{
+    int64_t v = cd.load();
+    while (v >= 0) {
+        if (cd.compare_exchange_weak(v, v - 1))
+            return v == 0;
+    }
+    return false;
+}
+template <typename T>
+inline cudaError_t dev_alloc(T **p, size_t bytes)
+{
+    if (injected_failure(g_fail_dev))
+        return cudaErrorMemoryAllocation;
+    return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+}
+template <typename T>
+inline cudaError_t dev_alloc_pool(T **p, size_t bytes, cudaMemPool_t pool, cudaStream_t st)
+{
+    if (injected_failure(g_fail_dev))
+        return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, st);
+}
+template <typename T>
+inline cudaError_t pinned_alloc(T **p, size_t bytes)
+{
+    if (injected_failure(g_fail_pin))
+        return cudaErrorMemoryAllocation;
+    return cudaMallocHost(reinterpret_cast<void **>(p), bytes);
+}
+
 #define GB2_CU(ctx, call)                                                                  \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \
@@ -179,6 +225,10 @@ int set_err(gb2_ctx *c, int code, const char *fmt, ...);
                                   "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
                                   __LINE__);                                               \
     } while (0)
+
+// Returns rc; when rc is an error, first waits for every stream of the
+// context, so a failed call leaves no work of its own in flight.
+int drain_on_error(gb2_ctx *c, int rc);
 
 int exec_init(Exec &x);
 void exec_free(Exec &x);

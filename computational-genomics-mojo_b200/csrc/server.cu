@@ -62,7 +62,7 @@ int ensure_host(HostBuf &b, size_t bytes)
     b.cap = 0;
     // pinning memory is slow: grow with headroom, rarely
     const size_t cap = std::max<size_t>(2 * bytes, 1 << 20);
-    if (cudaMallocHost(&b.p, cap) != cudaSuccess) {
+    if (pinned_alloc(&b.p, cap) != cudaSuccess) {
         cudaGetLastError();
         return GB2_ENOMEM;
     }
@@ -142,6 +142,7 @@ struct gb2_server {
     std::map<uint64_t, Req *> table;
     uint64_t next_ticket = 1;
     bool stopping = false;
+    bool hold = false;  // admission held (gb2_server_hold)
     std::thread th;
     gb2_server_stats st{};
     // device memory pool of the slots' buffers: they grow by stream-ordered
@@ -176,8 +177,19 @@ int64_t group_bytes(const Layout &l, const gb2_wfa_cfg &w, int sm_count)
     if (l.n_wfa) {
         const int g = gcd_i(w.x, gcd_i(w.o, w.e));
         const int64_t nslot = std::max(w.x / g, (w.o + w.e) / g) + 1 + 2 * (w.e / g + 1);
+        // the single-kernel design (tuning variants): rings per warp in flight
         const int64_t warps = std::min<int64_t>(l.n_wfa + 3, (int64_t)sm_count * 16);
-        b += warps * nslot * (((l.wfa_qmax + l.wfa_rmax + 5) + 31) & ~int64_t(31)) * 4;
+        const int64_t rings =
+            warps * nslot * (((l.wfa_qmax + l.wfa_rmax + 5) + 31) & ~int64_t(31)) * 4;
+        // the tiers: their queues, the suspended pairs' records of the two
+        // transitions, and the G tier's per-block rings
+        const WfaTierPlan pl = wfa_tier_plan(WfaParams{w.x, w.o, w.e, w.max_error},
+                                             l.wfa_qmax, l.wfa_rmax);
+        int64_t tiers = l.n_wfa * 24 + (int64_t)sm_count * pl.gring_block_bytes;
+        for (int t = 0; t < 2; ++t)
+            tiers += std::min<int64_t>(l.n_wfa, kTierDumpCap / pl.dump_stride[t]) *
+                     pl.dump_stride[t];
+        b += std::max(rings, tiers);
         b += l.n_wfa * 8 + kLenBuckets * 4;
     }
     return b;
@@ -369,7 +381,7 @@ void scheduler(gb2_server *s)
         // launch groups while an executor is free and the oldest request fits
         for (auto &up : s->slots) {
             Slot &sl = *up;
-            if (sl.busy || s->pending.empty())
+            if (sl.busy || s->pending.empty() || s->hold)
                 continue;
             Layout L;
             std::vector<Req *> take;
@@ -428,7 +440,7 @@ void scheduler(gb2_server *s)
                 busy |= up->busy;
                 free_slot |= !up->busy;
             }
-            if (free_slot && !s->pending.empty() &&
+            if (free_slot && !s->pending.empty() && !s->hold &&
                 s->st.inflight_bytes + s->pending.front()->need_alone <= s->cfg.hbm_budget_bytes)
                 return true;
             return s->stopping && s->pending.empty() && !busy;
@@ -471,7 +483,7 @@ int gb2_server_start(gb2_ctx *c, const gb2_server_cfg *cfg, gb2_server **out)
         auto sl = std::make_unique<Slot>();
         for (DevBuf *b : {&sl->d_in, &sl->d_out, &sl->x.keys, &sl->x.queue, &sl->x.counts,
                           &sl->x.seg, &sl->x.counters, &sl->x.scratch64, &sl->x.scratch32,
-                          &sl->x.work, &sl->x.errflag})
+                          &sl->x.work, &sl->x.errflag, &sl->x.tierq, &sl->x.dumps})
             b->pool = s->pool;
         if (exec_init(sl->x) != GB2_OK) {
             exec_free(sl->x);
@@ -622,6 +634,46 @@ int gb2_server_stats_get(gb2_server *s, gb2_server_stats *st)
     return GB2_OK;
 }
 
+int gb2_server_hold(gb2_server *s, int hold)
+{
+    if (!s)
+        return GB2_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stopping)
+            return GB2_ESTATE;
+        s->hold = hold != 0;
+    }
+    s->cv_sched.notify_one();
+    return GB2_OK;
+}
+
+int gb2_server_cancel(gb2_server *s, uint64_t ticket)
+{
+    if (!s)
+        return GB2_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->table.find(ticket);
+        if (it == s->table.end())
+            return GB2_EINVAL;
+        Req *rq = it->second;
+        if (rq->status != 1)
+            return GB2_ESTATE;  // running or done
+        for (auto p = s->pending.begin(); p != s->pending.end(); ++p)
+            if (*p == rq) {
+                s->pending.erase(p);
+                break;
+            }
+        rq->status = GB2_ECANCELED;
+        rq->t_done = Clock::now();
+        s->st.cancelled += 1;
+    }
+    s->cv_done.notify_all();
+    s->cv_sched.notify_one();  // the next queued request may fit now
+    return GB2_OK;
+}
+
 int gb2_server_stop(gb2_server *s)
 {
     if (!s)
@@ -629,6 +681,7 @@ int gb2_server_stop(gb2_server *s)
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stopping = true;
+        s->hold = false;  // stopping finishes every queued request
     }
     s->cv_sched.notify_all();
     if (s->th.joinable())

@@ -286,7 +286,7 @@ sw_band_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__r
 // kernel arguments rather than literals so that the multiply-adds using them
 // stay multiply-adds.
 struct Pack16Consts {
-    uint32_t one, x4, x128, x256, half;
+    uint32_t one, x4, x8, x32, x128, x256, half;
     uint32_t dm[4];  // (match - mismatch) << 18, 20, 22, 24
     uint32_t mmg2;   // mismatch - (go+ge) in both halves
     uint32_t neg_g2; // minus -(go+ge) in both halves, mod 2^32
@@ -324,10 +324,26 @@ __device__ __forceinline__ uint32_t seq_word16(const SeqView &s, int64_t off, in
 // the step lies inside the matrix (the common case); MASK = true zeroes the
 // first-maximum keys of cells past the query or reference end.  Returns the
 // packed row keys: low half row t, high half row t-1.
-template <int B, bool MASK>
+//
+// WIDE keys (scores up to 4094, bands 16..128): the key H*128 + column of the
+// narrow form needs H <= 511 and 2B+1 <= 128 columns.  The wide form keys a
+// cell as H*8 + (7 - h%8) (no carry between halves while H <= 8191), takes
+// the maximum over each group of 8 registers, and turns each group's maximum
+// into relu(gk - 8*base) with one DPX instruction, base = the best score of
+// the rows already resolved: a cell can only become the new best when
+// H > base, and then H - base <= 2*match (a row's maximum exceeds the
+// previous row's by at most `match`).  The group key
+//   (H - base) * 256 + (31 - group) * 8 + (7 - h%8)
+// fits 16 bits for match <= 127, and its maximum over the groups is the
+// first maximum of the half; group keys below 256 mean "nothing above base".
+// Per register this costs what the narrow key costs (one multiply-add and
+// half a 3-way max); the DPX relu, two logic ops and a multiply-add run once
+// per group.
+template <int B, bool MASK, bool WIDE>
 __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const uint32_t *eq,
                                                  const uint32_t *bw, uint32_t &e_last, int limL,
-                                                 int limH, const Pack16Consts &c)
+                                                 int limH, const Pack16Consts &c,
+                                                 uint32_t negbase8)
 {
     constexpr int NL = B + 1, R = NL;
     const uint32_t SENT = 0x0000C000u;
@@ -335,6 +351,7 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
     uint32_t el = __byte_perm(SENT, e_last, 0x5410);  // low: chain start; high: E'(t-1, B)
     uint32_t h0new = 0;
     uint32_t rk = 0, kpend = 0;
+    uint32_t gacc = 0, gpend = 0, g2pend = 0;  // WIDE: group maximum, pending keys
 #pragma unroll
     for (int h = 0; h < R; ++h) {
         const int k = h >> 4, j = h & 15, jj = h & 7;
@@ -356,21 +373,53 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
         Hr[h] = hn;
         hl = hn;
         el = e;
-        uint32_t key = hn * c.x128 + (((uint32_t)(127 - h)) | ((uint32_t)(127 - NL - h) << 16));
-        if (MASK)
-            key &= (h < limL ? 0x0000FFFFu : 0u) | (h < limH ? 0xFFFF0000u : 0u);
-        if (h & 1)
-            rk = __vimax3_u16x2(rk, kpend, key);
-        else
-            kpend = key;
+        if (!WIDE) {
+            uint32_t key =
+                hn * c.x128 + (((uint32_t)(127 - h)) | ((uint32_t)(127 - NL - h) << 16));
+            if (MASK)
+                key &= (h < limL ? 0x0000FFFFu : 0u) | (h < limH ? 0xFFFF0000u : 0u);
+            if (h & 1)
+                rk = __vimax3_u16x2(rk, kpend, key);
+            else
+                kpend = key;
+        } else {
+            const int i = h & 7, g = h >> 3;
+            const uint32_t t8 = 7u - (uint32_t)i;
+            uint32_t key = hn * c.x8 + (t8 | (t8 << 16));
+            if (MASK)
+                key &= (h < limL ? 0x0000FFFFu : 0u) | (h < limH ? 0xFFFF0000u : 0u);
+            if (i == 0)
+                gacc = key;
+            else if (i & 1)
+                gpend = key;
+            else
+                gacc = __vimax3_u16x2(gacc, gpend, key);
+            if (i == 7 || h == R - 1) {
+                if (i & 1)
+                    gacc = __vimax3_u16x2(gacc, gpend, gpend);
+                const uint32_t ck = __viaddmax_s16x2_relu(gacc, negbase8, 0u);
+                const uint32_t cg = (uint32_t)((31 - g) * 8) * 0x00010001u;
+                const uint32_t k2 = (ck & 0xFFF8FFF8u) * c.x32 + ((ck & 0x00070007u) | cg);
+                if (g & 1)
+                    rk = __vimax3_u16x2(rk, g2pend, k2);
+                else
+                    g2pend = k2;
+            }
+        }
     }
-    if ((R - 1) % 2 == 0)
-        rk = __vimax3_u16x2(rk, kpend, kpend);
+    if (!WIDE) {
+        if ((R - 1) % 2 == 0)
+            rk = __vimax3_u16x2(rk, kpend, kpend);
+    } else {
+        constexpr int NG = (R + 7) / 8;
+        if ((NG - 1) % 2 == 0)
+            rk = __vimax3_u16x2(rk, g2pend, g2pend);
+    }
     e_last = el;
     return rk;
 }
 
-template <int B>
+template <int B, bool WIDE>
 __global__ void __launch_bounds__(128)
 sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_result *__restrict__ out)
 {
@@ -382,7 +431,8 @@ sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_resul
     constexpr int BW0 = NL / 16;        // first word of columns B+1.. (offset one column)
     constexpr int NBW = B / 16;         // shifted words of the previous row
     constexpr int RW0 = NE - B / 16;    // 16-base word entering the window at t = 0
-    static_assert(W <= 127, "column index must fit the key");
+    static_assert(WIDE || W <= 127, "column index must fit the narrow key");
+    static_assert(!WIDE || (R + 7) / 8 <= 32, "group index must fit the wide key");
     static_assert(NL % 16 == 1 && BW0 + NBW < NE, "word layout");
 
     int64_t n;
@@ -430,6 +480,8 @@ sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_resul
             uint32_t e_last = SENT;
             uint32_t saved_lowkey = 0, bestkey = 0, thr = 127;
             int32_t bq = 0;
+            // WIDE: best score, its column, and the base the saved key was taken at
+            int32_t best = 0, bcol = 0, base_prev = 0;
             uint32_t qw = 0, rw = 0;
             uint32_t qn = seq_word16(q, qoff, 0), rn = seq_word16(r, roff, RW0);  // next words
             const int steps = qlen > 0 ? qlen + 1 : 0;
@@ -481,27 +533,55 @@ sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_resul
                     if (t >= 1 && t - 1 < qlen)
                         limH = max(0, min(R, rlen - (t - 1 - B + NL)));
                 }
-                const uint32_t rk = full ? pack16_cells<B, false>(Hr, eq, bw, e_last, 0, 0, c)
-                                         : pack16_cells<B, true>(Hr, eq, bw, e_last, limL, limH, c);
-                // row t-1 is complete: its first half came one step earlier; a key
-                // above thr = bestkey | 127 has a larger H than the best so far
-                const uint32_t rowkey = max(saved_lowkey, rk >> 16);
-                if (rowkey > thr) {
-                    thr = rowkey | 127u;
-                    bestkey = rowkey;
-                    bq = t - 1;
+                // WIDE keys are relative to the best score of rows <= t-2
+                const uint32_t negbase8 = (uint32_t)(uint16_t)(-8 * best) * 0x00010001u;
+                const uint32_t rk =
+                    full ? pack16_cells<B, false, WIDE>(Hr, eq, bw, e_last, 0, 0, c, negbase8)
+                         : pack16_cells<B, true, WIDE>(Hr, eq, bw, e_last, limL, limH, c,
+                                                       negbase8);
+                if (!WIDE) {
+                    // row t-1 is complete: its first half came one step earlier; a key
+                    // above thr = bestkey | 127 has a larger H than the best so far
+                    const uint32_t rowkey = max(saved_lowkey, rk >> 16);
+                    if (rowkey > thr) {
+                        thr = rowkey | 127u;
+                        bestkey = rowkey;
+                        bq = t - 1;
+                    }
+                    saved_lowkey = rk & 0xFFFFu;
+                } else {
+                    // the saved low half of row t-1 was keyed against base_prev: rebase
+                    // it to this step's base; then the low half wins ties (its columns
+                    // come first)
+                    const uint32_t dsh = (uint32_t)(best - base_prev) << 8;
+                    const uint32_t sl = saved_lowkey >= dsh + 256u ? saved_lowkey - dsh : 0u;
+                    const uint32_t hi = rk >> 16;
+                    const int32_t dl = (int32_t)(sl >> 8), dh = (int32_t)(hi >> 8);
+                    base_prev = best;
+                    if (dl > 0 || dh > 0) {
+                        if (dl >= dh) {
+                            best += dl;
+                            bcol = 255 - (int32_t)(sl & 255u);
+                        } else {
+                            best += dh;
+                            bcol = NL + 255 - (int32_t)(hi & 255u);
+                        }
+                        bq = t - 1;
+                    }
+                    saved_lowkey = rk & 0xFFFFu;
                 }
-                saved_lowkey = rk & 0xFFFFu;
 #pragma unroll
                 for (int i = 0; i < NE; ++i)
                     ep[i] = eq[i];
             }
-            const int32_t best = (int32_t)(bestkey >> 7);
-            const int32_t bc = 127 - (int32_t)(bestkey & 127u);
+            if (!WIDE) {
+                best = (int32_t)(bestkey >> 7);
+                bcol = 127 - (int32_t)(bestkey & 127u);
+            }
             gb2_sw_result res;
             res.score = best;
             res.query_end = best > 0 ? bq : 0;
-            res.ref_end = best > 0 ? bq - B + bc : 0;
+            res.ref_end = best > 0 ? bq - B + bcol : 0;
             out[pi] = res;
         }
         if (!queue_counter)
@@ -577,6 +657,101 @@ sw_literal_kernel(SeqView q, SeqView r, SwParams p, int32_t band, const int32_t 
     }
 }
 
+// Naive baseline (GB2_FLAG_NAIVE): one 128-thread block per pair, launched
+// over all pairs in input order with no planning, as the reference's
+// launch_banded_sw does (genomics/gpu/align_gpu.mojo:482-492) -- but computing
+// the CPU recurrence exactly.  Cell (qi, j) of the band runs at step
+// s = 2*qi + j: its diag (qi-1, j) ran at s-2, its up (qi-1, j+1) and left
+// (qi, j-1) at s-1, so the cells of one step (one parity of j) are
+// independent and one row of H and E per band column, in shared memory, holds
+// every value a step reads; a barrier separates the steps.  Skipped cells
+// (reference position outside [0, rlen)) hold 0 as the reference's reset rows
+// do (align_cpu.mojo:261-268).  int32 values (the host bounds every score).
+__global__ void __launch_bounds__(128)
+sw_naive_kernel(SeqView q, SeqView r, SwParams p, int32_t band, const int32_t *__restrict__ bands,
+                int64_t n, gb2_sw_result *__restrict__ out)
+{
+    extern __shared__ int32_t nsm[];
+    __shared__ unsigned long long red[4];
+    const int64_t pi = blockIdx.x;
+    if (pi >= n)
+        return;
+    const int32_t b = bands ? bands[pi] : band;
+    const int32_t W = 2 * b + 1;
+    int32_t *const Hs = nsm;
+    int32_t *const Es = nsm + W;
+    const int32_t qlen = (int32_t)q.lengths[pi], rlen = (int32_t)r.lengths[pi];
+    const uint64_t *qw = q.packed + (q.offsets[pi] - q.word_base);
+    const uint64_t *rw = r.packed + (r.offsets[pi] - r.word_base);
+    for (int32_t j = threadIdx.x; j < W; j += blockDim.x) {
+        Hs[j] = 0;
+        Es[j] = 0;
+    }
+    __syncthreads();
+    unsigned long long best = 0;  // H << 42 | (2^21-1 - qi) << 21 | (2^21-1 - j)
+    const int32_t steps = qlen > 0 ? 2 * (qlen - 1) + W : 0;
+    const int32_t goe = p.go + p.ge;
+    for (int32_t st = 0; st < steps; ++st) {
+        // active columns: parity of st, qi = (st - j) / 2 in [0, qlen)
+        const int32_t jlo = max(st & 1, st - 2 * (qlen - 1));
+        const int32_t jhi = min(W - 1, st);
+        for (int32_t j = jlo + 2 * (int32_t)threadIdx.x; j <= jhi; j += 2 * (int32_t)blockDim.x) {
+            const int32_t qi = (st - j) >> 1;
+            const int32_t ri = qi - b + j;
+            int32_t h = 0, e = 0;
+            if (ri >= 0 && ri < rlen) {
+                const int32_t qb = (int32_t)((qw[qi >> 5] >> (62 - 2 * (qi & 31))) & 3u);
+                const int32_t rb = (int32_t)((rw[ri >> 5] >> (62 - 2 * (ri & 31))) & 3u);
+                const int32_t sub = qb == rb ? p.match : p.mismatch;
+                const int32_t h_diag = Hs[j];
+                const int32_t h_up = j + 1 < W ? Hs[j + 1] : 0;
+                const int32_t h_left = j > 0 ? Hs[j - 1] : 0;
+                const int32_t e1 = j > 0 ? Es[j - 1] + p.ge : -1000000;
+                e = max(e1, h_up + goe);
+                h = max(max(h_diag + sub, e), max(h_left + goe, 0));
+                if (h > 0) {
+                    const unsigned long long key =
+                        ((unsigned long long)h << 42) |
+                        ((unsigned long long)(0x1FFFFF - qi) << 21) |
+                        (unsigned long long)(0x1FFFFF - j);
+                    best = key > best ? key : best;
+                }
+            }
+            Hs[j] = h;
+            Es[j] = e;
+        }
+        __syncthreads();
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, off);
+        best = o > best ? o : best;
+    }
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i)
+            best = red[i] > best ? red[i] : best;
+        sw_store(out, pi, best, b);
+    }
+}
+
+cudaError_t launch_sw_naive(SeqView q, SeqView r, SwParams p, int32_t band, const int32_t *bands,
+                            int32_t max_band, int64_t n, gb2_sw_result *out, cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    if (n > 0x7fffffff || max_band > kSwNaiveMaxBand)
+        return cudaErrorInvalidValue;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        sw_naive_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)(2 * (2 * kSwNaiveMaxBand + 1) * sizeof(int32_t)));
+    (void)attr;
+    const size_t smem = (size_t)2 * (2 * (size_t)max_band + 1) * sizeof(int32_t);
+    sw_naive_kernel<<<(unsigned)n, 128, smem, st>>>(q, r, p, band, bands, n, out);
+    return cudaGetLastError();
+}
+
 template <int B, int G, int K>
 static cudaError_t launch_band(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *out,
                                int grid, cudaStream_t st)
@@ -602,19 +777,23 @@ static int occ_band()
     return nb > 0 ? nb : 1;
 }
 
-template <int B>
+template <int B, bool WIDE>
 static int occ_pack16()
 {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sw_pack16_kernel<B>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sw_pack16_kernel<B, WIDE>, 128, 0);
     return nb > 0 ? nb : 1;
 }
 
 int sw_blocks_per_sm(int band_class, int variant)
 {
     switch (band_class) {
-    case 16 | kPack16: return occ_pack16<16>();
-    case 32 | kPack16: return occ_pack16<32>();
+    case 16 | kPack16: return occ_pack16<16, false>();
+    case 32 | kPack16: return occ_pack16<32, false>();
+    case 16 | kPackWide: return occ_pack16<16, true>();
+    case 32 | kPackWide: return occ_pack16<32, true>();
+    case 64 | kPackWide: return occ_pack16<64, true>();
+    case 128 | kPackWide: return occ_pack16<128, true>();
     case 16: return variant == 1 ? occ_band<16, 2, 17>() : occ_band<16, 1, 33>();
     case 32:
         return variant == 1 ? occ_band<32, 2, 33>()
@@ -630,7 +809,11 @@ int sw_pairs_per_block(int band_class, int variant)
     int G = 1;
     switch (band_class) {
     case 16 | kPack16:
-    case 32 | kPack16: return 128;
+    case 32 | kPack16:
+    case 16 | kPackWide:
+    case 32 | kPackWide:
+    case 64 | kPackWide:
+    case 128 | kPackWide: return 128;
     case 16: G = variant == 1 ? 2 : 1; break;
     case 32: G = variant == 1 ? 2 : (variant == 2 ? 4 : 1); break;
     case 64: G = variant == 1 ? 4 : 2; break;
@@ -647,7 +830,11 @@ cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParam
 {
     switch (band_class) {
     case 16 | kPack16:
-    case 32 | kPack16: {
+    case 32 | kPack16:
+    case 16 | kPackWide:
+    case 32 | kPackWide:
+    case 64 | kPackWide:
+    case 128 | kPackWide: {
         int g = grid;
         if (g <= 0) {
             if (pl.seg || pl.n <= 0)
@@ -658,6 +845,8 @@ cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParam
         Pack16Consts c;
         c.one = 1;
         c.x4 = 4;
+        c.x8 = 8;
+        c.x32 = 32;
         c.x128 = 128;
         c.x256 = 256;
         c.half = 0x80000000u;
@@ -667,10 +856,14 @@ cudaError_t launch_sw(int band_class, int variant, SeqView q, SeqView r, SwParam
         c.neg_g2 = 0u - gg * 0x00010001u;
         c.ge2 = (uint32_t)(uint16_t)p.ge * 0x00010001u;
         c.ng2 = (uint32_t)(uint16_t)gg * 0x00010001u;
-        if (band_class == (16 | kPack16))
-            sw_pack16_kernel<16><<<g, 128, 0, st>>>(q, r, c, pl, out);
-        else
-            sw_pack16_kernel<32><<<g, 128, 0, st>>>(q, r, c, pl, out);
+        switch (band_class) {
+        case 16 | kPack16: sw_pack16_kernel<16, false><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        case 32 | kPack16: sw_pack16_kernel<32, false><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        case 16 | kPackWide: sw_pack16_kernel<16, true><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        case 32 | kPackWide: sw_pack16_kernel<32, true><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        case 64 | kPackWide: sw_pack16_kernel<64, true><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        default: sw_pack16_kernel<128, true><<<g, 128, 0, st>>>(q, r, c, pl, out); break;
+        }
         return cudaGetLastError();
     }
     case 16:

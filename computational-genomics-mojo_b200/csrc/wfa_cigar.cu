@@ -198,7 +198,7 @@ static int wfa_cigar_run(gb2_ctx *c, SeqView qv, SeqView rv, const int64_t *h_ql
 
 extern "C" {
 
-int gb2_wfa_cigar(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
+static int gb2_wfa_cigar_impl(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
                   int64_t n, int32_t *cost, uint32_t *runs, int64_t runs_cap,
                   int64_t *run_offsets, int flags)
 {
@@ -230,7 +230,14 @@ int gb2_wfa_cigar(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_
                          runs, runs_cap, run_offsets, flags);
 }
 
-int gb2_wfa_cigar_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen,
+int gb2_wfa_cigar(gb2_ctx *c, const gb2_batch *q, const gb2_batch *r, const gb2_wfa_cfg *cfg,
+                  int64_t n, int32_t *cost, uint32_t *runs, int64_t runs_cap,
+                  int64_t *run_offsets, int flags)
+{
+    return drain_on_error(c, gb2_wfa_cigar_impl(c, q, r, cfg, n, cost, runs, runs_cap, run_offsets, flags));
+}
+
+static int gb2_wfa_cigar_pair_impl(gb2_ctx *c, const uint64_t *q_words, int64_t qlen,
                        const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
                        int32_t *cost, char *cigar, int64_t cap)
 {
@@ -270,6 +277,13 @@ int gb2_wfa_cigar_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen,
     }
     cigar[pos] = 0;
     return GB2_OK;
+}
+
+int gb2_wfa_cigar_pair(gb2_ctx *c, const uint64_t *q_words, int64_t qlen,
+                       const uint64_t *r_words, int64_t rlen, const gb2_wfa_cfg *cfg,
+                       int32_t *cost, char *cigar, int64_t cap)
+{
+    return drain_on_error(c, gb2_wfa_cigar_pair_impl(c, q_words, qlen, r_words, rlen, cfg, cost, cigar, cap));
 }
 
 }  // extern "C"

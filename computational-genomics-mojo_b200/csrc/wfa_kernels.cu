@@ -247,7 +247,14 @@ __device__ __forceinline__ int32_t wfa_align_pair(const SeqView &q, const SeqVie
     int32_t *const hdr = reinterpret_cast<int32_t *>(hrec);
     int64_t hcur = 3 * (int64_t)hsteps;  // next free 4-byte word of the record
     bool overrun = false, need32 = false;
-    if (qlen == 0 && rlen == 0) {
+    const int64_t ql64 = q.lengths[pi], rl64 = r.lengths[pi];
+    if (ql64 < 0 || rl64 < 0 || ql64 + rl64 + 5 > slot_width) {
+        // a length the caller's bounds did not cover (negative, 2^31 or more, or
+        // past the rings): cost -2 and the error flag
+        if (tt == 0)
+            atomicOr(err_flag, 1);
+        result = -2;
+    } else if (qlen == 0 && rlen == 0) {
         result = 0;
     } else if ((int64_t)qlen + rlen + 5 > slot_width) {
         if (tt == 0)

@@ -16,8 +16,8 @@ INCLUDE = os.path.join(REPO_ROOT, "include")
 LIB = os.path.join(LIBDIR, "libgenomics_b200.so")
 SYNTH = os.path.join(LIBDIR, "libgenomics_synth.so")
 
-CU_SOURCES = ["api.cu", "sw_kernels.cu", "wfa_kernels.cu", "wfa_cigar.cu", "nw.cu", "noalloc.cu",
-              "server.cu", "pack.cu"]
+CU_SOURCES = ["api.cu", "sw_kernels.cu", "wfa_kernels.cu", "wfa_tiers.cu", "wfa_cigar.cu",
+              "nw.cu", "noalloc.cu", "server.cu", "pack.cu", "multi.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -25,12 +25,16 @@ GB2_ETIMEOUT = -6
 GB2_ESTATE = -7
 GB2_EKERNEL = -8
 GB2_ESCRATCH = -9
+GB2_ECANCELED = -10
+GB2_ALLOC_DEVICE = 1
+GB2_ALLOC_PINNED = 2
 
 FLAG_PLAIN = 0x0
 FLAG_BATCHED = 0x1
 FLAG_INT32 = 0x2
 FLAG_GENERIC = 0x4
 FLAG_GRAPH = 0x8  # capture resident calls into a CUDA graph and replay it
+FLAG_NAIVE = 0x10  # baseline: one thread block per pair, input order, no planning
 
 
 class SwCfg(ctypes.Structure):
@@ -78,7 +82,8 @@ class ServerCfg(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", c_i64), ("completed", c_i64), ("failed", c_i64),
                 ("pairs_completed", c_i64), ("groups_launched", c_i64),
-                ("inflight_bytes", c_i64), ("peak_inflight_bytes", c_i64)]
+                ("inflight_bytes", c_i64), ("peak_inflight_bytes", c_i64),
+                ("cancelled", c_i64)]
 
 
 # (name, restype, argtypes) for every entry point of include/genomics_b200.h
@@ -110,12 +115,21 @@ SIGNATURES = [
      [vp, vp, c_i64, vp, c_i64, P(WfaCfg), P(c_i32), ctypes.c_char_p, c_i64]),
     ("gb2_wfa_affine_noalloc", ctypes.c_int,
      [vp, c_i64, vp, vp, vp, c_i64, vp, vp, c_i64, c_i64, P(WfaCfg), c_i64, vp, vp]),
+    ("gb2_partition_pairs", ctypes.c_int,
+     [vp, vp, vp, c_i32, ctypes.c_int, c_i64, ctypes.c_int, vp]),
+    ("gb2_sw_banded_multi", ctypes.c_int,
+     [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, P(SwCfg), vp, c_i64, vp, ctypes.c_int]),
+    ("gb2_wfa_affine_multi", ctypes.c_int,
+     [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, P(WfaCfg), c_i64, vp, ctypes.c_int]),
     ("gb2_server_start", ctypes.c_int, [vp, P(ServerCfg), P(vp)]),
     ("gb2_server_submit", ctypes.c_int, [vp, P(Request), P(ctypes.c_uint64)]),
     ("gb2_server_poll", ctypes.c_int, [vp, ctypes.c_uint64, P(ctypes.c_int)]),
     ("gb2_server_wait", ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_double)]),
     ("gb2_server_stats_get", ctypes.c_int, [vp, P(ServerStats)]),
     ("gb2_server_stop", ctypes.c_int, [vp]),
+    ("gb2_server_hold", ctypes.c_int, [vp, ctypes.c_int]),
+    ("gb2_server_cancel", ctypes.c_int, [vp, ctypes.c_uint64]),
+    ("gb2_debug_fail_alloc", ctypes.c_int, [ctypes.c_int, c_i64]),
     ("gb2_host_alloc", ctypes.c_int, [c_i64, P(vp)]),
     ("gb2_host_free", ctypes.c_int, [vp]),
     ("gb2_timer_start", ctypes.c_int, [vp]),

@@ -45,6 +45,12 @@ class PendingRequest:
         check(self.server.L.gb2_server_poll(self.server.handle, self.ticket, ctypes.byref(d)))
         return bool(d.value)
 
+    def cancel(self):
+        """Takes the request out of the queue if it has not started (gb2_server_cancel);
+        its wait then raises GenomicsError(GB2_ECANCELED)."""
+        check(self.server.L.gb2_server_cancel(self.server.handle, self.ticket),
+              self.server.dev.ctx)
+
     def wait(self, timeout_ms: int = -1):
         """Blocks until done; returns (sw_results, wfa_costs) and sets latency_ms."""
         if self.status is None:
@@ -94,6 +100,10 @@ class AlignmentServer:
               self.dev.ctx)
         keep = (qp, qo, ql, rp, ro, rl, k, b)
         return PendingRequest(self, t.value, keep, sw_out, wfa_out, k)
+
+    def hold(self, on: bool = True):
+        """Holds (or resumes) admission: queued requests wait, running groups finish."""
+        check(self.L.gb2_server_hold(self.handle, 1 if on else 0), self.dev.ctx)
 
     def stats(self) -> dict:
         st = ServerStats()

@@ -40,6 +40,7 @@ extern "C" {
 #define GB2_ESTATE (-7)      /* wrong state (server not running, ...) */
 #define GB2_EKERNEL (-8)     /* a kernel reported an internal error flag */
 #define GB2_ESCRATCH (-9)    /* request too large for the fixed no-allocation scratch */
+#define GB2_ECANCELED (-10)  /* a served request was cancelled before it ran */
 
 /* ---- configuration and result structs ------------------------------------- */
 
@@ -80,6 +81,10 @@ typedef struct gb2_batch gb2_batch;
                                   work into a CUDA graph on the second call with the same
                                   shape (batches, scoring, n_pairs, flags) and replay it on
                                   later ones; results are those of the eager launches */
+#define GB2_FLAG_NAIVE 0x10    /* gb2_sw_banded / gb2_wfa_affine: the baseline the batched
+                                  path is measured against -- one launch, one thread block
+                                  per pair in input order, no planning, as the reference's
+                                  launchers do (genomics/gpu/align_gpu.mojo:482-492, :524-534) */
 /* Tuning fields (0 = the library's choice): bits 8-15 select a kernel
  * variant; bits 16-23 set how many chunks the *_host entry points split a
  * batch into for their copy/compute pipeline. */
@@ -237,8 +242,9 @@ int gb2_wfa_cigar_pair(gb2_ctx *ctx, const uint64_t *q_words, int64_t qlen,
  * it until the process exits.  max_qlen / max_rlen bound the lengths: a
  * request whose rings ((max(x,o+e)/g + 1 + 2(e/g + 1)) slots x
  * (max_qlen + max_rlen + 5) int32 per warp, g = gcd(x, o, e)) leave room for
- * fewer than four warps returns GB2_ESCRATCH; a pair longer than stated gets
- * cost -2 and the call returns GB2_EINVAL.  Blocking on `stream` (a
+ * fewer than four warps returns GB2_ESCRATCH; a pair longer than stated, or
+ * with a negative length or one of 2^31 or more, gets cost -2 and the call
+ * returns GB2_EINVAL.  Blocking on `stream` (a
  * cudaStream_t; NULL = the legacy default stream).  The first call on a
  * device looks up the array's device address, so make it before any stream
  * capture.  All calls share the array: calls that overlap on the GPU race. */
@@ -250,6 +256,35 @@ int gb2_wfa_affine_noalloc(const uint64_t *q_packed, int64_t q_words,
                            int64_t max_qlen, int64_t max_rlen,
                            const gb2_wfa_cfg *cfg, int64_t n_pairs,
                            int32_t *out_cost, void *stream);
+
+/* ---- one pair list over several devices --------------------------------------------
+ * Pairs are independent (the reference gives each its own thread block,
+ * genomics/gpu/align_gpu.mojo:80), so a list splits into contiguous slices with
+ * no exchange step.  gb2_partition_pairs (host only, no device needed) writes
+ * n_parts + 1 bounds: part k is pairs [bounds[k], bounds[k+1]), cut where the
+ * cumulative work reaches k/n_parts of the total -- kind 0 Smith-Waterman
+ * cells qlen * (2 * band + 1) (bands per pair, or `band`), kind 1 WFA
+ * max(qlen, rlen)^2 (the visited cells grow with the square of the cost) --
+ * plus a fixed share per pair.  The *_multi entry points run slice k on
+ * ctxs[k] (each context on its own device, or several on one) from the
+ * caller's host arrays, on one host thread per context, and write each
+ * slice's results into `out` at its offset, so `out` is in input order.  The
+ * first failing slice's status is returned. */
+int gb2_partition_pairs(const int64_t *q_lengths, const int64_t *r_lengths, const int32_t *bands,
+                        int32_t band, int kind, int64_t n_pairs, int n_parts, int64_t *bounds);
+int gb2_sw_banded_multi(gb2_ctx *const *ctxs, int n_ctx,
+                        const uint64_t *q_packed, const int64_t *q_offsets,
+                        const int64_t *q_lengths,
+                        const uint64_t *r_packed, const int64_t *r_offsets,
+                        const int64_t *r_lengths,
+                        const gb2_sw_cfg *cfg, const int32_t *bands, int64_t n_pairs,
+                        gb2_sw_result *out, int flags);
+int gb2_wfa_affine_multi(gb2_ctx *const *ctxs, int n_ctx,
+                         const uint64_t *q_packed, const int64_t *q_offsets,
+                         const int64_t *q_lengths,
+                         const uint64_t *r_packed, const int64_t *r_offsets,
+                         const int64_t *r_lengths,
+                         const gb2_wfa_cfg *cfg, int64_t n_pairs, int32_t *out_cost, int flags);
 
 /* ---- serving: continuous batching of alignment requests ----------------------------
  * A request is a batch of pairs; each pair is Smith-Waterman or WFA.  Requests
@@ -287,6 +322,7 @@ typedef struct {
 typedef struct {
     int64_t submitted, completed, failed, pairs_completed, groups_launched;
     int64_t inflight_bytes, peak_inflight_bytes;
+    int64_t cancelled;
 } gb2_server_stats;
 
 typedef struct gb2_server gb2_server;
@@ -303,6 +339,13 @@ int gb2_server_poll(gb2_server *srv, uint64_t ticket, int *done);
    results written.  The ticket is released once reported done. */
 int gb2_server_wait(gb2_server *srv, uint64_t ticket, int timeout_ms, double *latency_ms);
 int gb2_server_stats_get(gb2_server *srv, gb2_server_stats *st);
+/* Hold admission (hold = 1): queued requests stay queued, groups already on
+   the GPU finish; hold = 0 resumes.  gb2_server_stop lifts a hold. */
+int gb2_server_hold(gb2_server *srv, int hold);
+/* Cancel a queued request: it leaves the queue without running, and its wait
+   returns GB2_ECANCELED.  A request already on the GPU, or done, cannot be
+   cancelled (GB2_ESTATE); an unknown ticket is GB2_EINVAL. */
+int gb2_server_cancel(gb2_server *srv, uint64_t ticket);
 /* Finish every queued and running request, then stop the thread. */
 int gb2_server_stop(gb2_server *srv);
 
@@ -339,6 +382,17 @@ int gb2_autotune(gb2_ctx *ctx, int kind, const gb2_batch *q, const gb2_batch *r,
                  int64_t n_pairs, int reps, gb2_tune_result *out);
 int gb2_tune_set(gb2_ctx *ctx, int kind, int band_class, int variant);
 int gb2_tune_get(gb2_ctx *ctx, int kind, int band_class, int *variant);
+
+/* ---- failure injection (testing) ---------------------------------------------------
+ * No counterpart in the reference (its only failure report is WFA's -1,
+ * genomics/cpu/align_cpu.mojo:226).  Arms a countdown: the nth device
+ * (GB2_ALLOC_DEVICE) or pinned host (GB2_ALLOC_PINNED) allocation the library
+ * makes from now on (0 = the next one) fails as if out of memory; the entry
+ * point that made it returns GB2_ENOMEM after waiting for its streams, and the
+ * context stays usable.  nth < 0 disarms.  Process-wide. */
+#define GB2_ALLOC_DEVICE 1
+#define GB2_ALLOC_PINNED 2
+int gb2_debug_fail_alloc(int kind, int64_t nth);
 
 /* ---- pinned host memory -----------------------------------------------------------
  * Page-locked host allocations: SequenceBatch arrays built here reach the

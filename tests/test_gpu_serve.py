@@ -132,3 +132,30 @@ def test_empty_request(device):
     with AlignmentServer(device) as srv:
         sw, wfa = srv.submit(e, e, SWC, WFAConfig(4, 6, 2, 10)).wait(10_000)
         assert sw.size == 0 and wfa.size == 0
+
+
+def test_long_wfa_pairs_alone_and_in_the_mix(device, oracle):
+    """Requests holding 8-20 kbp WFA pairs at up to 15% divergence (the pairs that
+    climb to the largest WFA tiers and to int32 rings) give the same costs alone
+    and mixed with short requests in flight, and equal the oracle."""
+    q, r, bands, kinds = synth.generate(4, 4000, seed=808)
+    lmax = np.maximum(q.lengths, r.lengths)
+    longs = np.nonzero((kinds == WFA) & (lmax >= 8000))[0][:6]
+    shorts = np.nonzero(lmax <= 1500)[0][:400]
+    assert longs.size == 6
+    wcfg = WFAConfig(4, 6, 2, synth.wfa_max_error_cover(q, r, 4, 6, 2))
+    big = (_subset(q, longs), _subset(r, longs), bands[longs], kinds[longs])
+    exp_big = _expected(oracle, big, wcfg)
+    small = [(_subset(q, shorts[i::4]), _subset(r, shorts[i::4]), bands[shorts[i::4]],
+              kinds[shorts[i::4]]) for i in range(4)]
+    with AlignmentServer(device, hbm_budget_bytes=16 << 30, max_inflight_groups=4) as srv:
+        alone = srv.submit(big[0], big[1], SWC, wcfg, kinds=big[3], bands=big[2]).wait(600_000)
+        _check(alone, exp_big, big[3], "long pairs alone")
+        prs = [srv.submit(s[0], s[1], SWC, wcfg, kinds=s[3], bands=s[2]) for s in small[:2]]
+        pb = srv.submit(big[0], big[1], SWC, wcfg, kinds=big[3], bands=big[2])
+        prs += [srv.submit(s[0], s[1], SWC, wcfg, kinds=s[3], bands=s[2]) for s in small[2:]]
+        mixed = pb.wait(600_000)
+        assert (mixed[1] == alone[1]).all()
+        _check(mixed, exp_big, big[3], "long pairs in the mix")
+        for s, pr in zip(small, prs):
+            _check(pr.wait(600_000), _expected(oracle, s, wcfg), s[3], "short requests")

@@ -196,6 +196,49 @@ def test_packed_int16_path_matches_int32_and_oracle(device, oracle, band):
     assert_same(device.sw_banded(q, r, cfg, flags=FLAG_INT32), ref, "reads int32")
 
 
+@pytest.mark.parametrize("band", [16, 32, 64, 128])
+def test_packed_wide_keys_match_int32_and_oracle(device, oracle, band):
+    """Pairs whose scores pass 511 (the narrow keys' limit) but stay within
+    match * (min(qlen, rlen) + 1) <= 4094 take the packed kernel with group keys;
+    GB2_FLAG_INT32 forces the int32 register kernels.  Both equal the oracle,
+    including first-maximum ties across groups and halves and rows past either
+    end."""
+    rng = random.Random(band * 13)
+    q, r = _random_pairs(rng, 600, 2000, "ACGTN")
+    # similar pairs reach large scores; repeats make equal maxima in many columns
+    reps = ["ACGT" * rng.randint(100, 450) for _ in range(40)]
+    q2 = SequenceBatch.from_strings(reps + [s[:rng.randint(300, len(s))] for s in reps])
+    r2 = SequenceBatch.from_strings([s[rng.randint(0, 20):] for s in reps] + reps)
+    for qq, rr in ((q, r), (q2, r2)):
+        for cfg in (AlignConfig(2, -4, -4, -2, band), AlignConfig(1, -1, 0, -1, band),
+                    AlignConfig(3, -2, -6, -1, band), AlignConfig(2, -8, -2, -1, band)):
+            ref = oracle_sw(oracle, qq, rr, cfg)
+            for batched in (False, True):
+                assert_same(device.sw_banded(qq, rr, cfg, batched=batched), ref,
+                            f"{cfg} wide packed batched={batched}")
+            assert_same(device.sw_banded(qq, rr, cfg, flags=FLAG_INT32), ref, f"{cfg} int32")
+
+
+def test_packed_wide_key_bounds(device, oracle):
+    """Pairs on both sides of the wide keys' score bound (match * (min + 1) =
+    4094 at match 2: min length 2046), mixed bands per pair."""
+    rng = random.Random(4094)
+    qs, rs, bands = [], [], []
+    for L in (2044, 2045, 2046, 2047, 2048, 3000):
+        for _ in range(4):
+            s = "".join(rng.choice("ACGT") for _ in range(L))
+            qs.append(s)
+            rs.append(s[:L // 2] + "G" + s[L // 2 + 1:])
+            bands.append(rng.choice([16, 32, 64, 128]))
+    q, r = SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+    b = np.array(bands, np.int32)
+    ref = oracle_sw(oracle, q, r, CFG0, bands=b)
+    assert (ref[0] > 4000).any()
+    for batched in (False, True):
+        assert_same(device.sw_banded(q, r, CFG0, bands=b, batched=batched), ref,
+                    f"bounds batched={batched}")
+
+
 def test_variants_agree(device, oracle):
     q, r, bands, _ = synth.generate(3, 3000, seed=77)
     ref = oracle_sw(oracle, q, r, CFG0, bands=bands)

@@ -68,3 +68,43 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(device):
     # rings for 4 warps of 9 x 600k int32 each exceed the 32 MiB scratch
     assert L.gb2_wfa_affine_noalloc(*args(300_000, 300_000)) == _lib.GB2_ESCRATCH
     assert L.gb2_strerror(_lib.GB2_ESCRATCH) == b"request exceeds the fixed no-allocation scratch"
+
+
+def test_noalloc_flags_pairs_longer_than_declared(device):
+    """A pair longer than the stated bounds gets cost -2 and the call returns
+    GB2_EINVAL; the next call with the right bounds is clean (the shared header
+    was cleared) and equals the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    import random
+    rng = random.Random(11)
+    rand = lambda n: "".join(rng.choice("ACGT") for _ in range(n))
+    qs = [rand(rng.randint(150, 240)) for _ in range(8)] + [rand(2000)]
+    rs = [s[:50] + "T" + s[51:] for s in qs]
+    from genomics_b200 import SequenceBatch
+    q, r = SequenceBatch.from_strings(qs), SequenceBatch.from_strings(rs)
+    cfg = WFAConfig(4, 6, 2, 4000)
+    want = device.wfa_affine(q, r, cfg)
+    qp, qo, ql = _device_copies(torch, q)
+    rp, ro, rl = _device_copies(torch, r)
+    n = len(qs)
+    out = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    c = _lib.WfaCfg(4, 6, 2, 4000)
+    L = _lib.lib()
+
+    def call(mq, mr):
+        out.fill_(-7)
+        rc = L.gb2_wfa_affine_noalloc(
+            ctypes.c_void_p(qp.data_ptr()), qp.numel(), ctypes.c_void_p(qo.data_ptr()),
+            ctypes.c_void_p(ql.data_ptr()), ctypes.c_void_p(rp.data_ptr()), rp.numel(),
+            ctypes.c_void_p(ro.data_ptr()), ctypes.c_void_p(rl.data_ptr()), mq, mr,
+            ctypes.byref(c), n, ctypes.c_void_p(out.data_ptr()), None)
+        torch.cuda.synchronize()
+        return rc, out.cpu().numpy()
+
+    rc, got = call(250, 250)  # the last pair is 2,000 bases: longer than declared
+    assert rc == _lib.GB2_EINVAL
+    assert got[-1] == -2
+    assert (got[:-1] == want[:-1]).all()
+    rc, got = call(int(q.lengths.max()), int(r.lengths.max()))
+    assert rc == _lib.GB2_OK
+    assert (got == want).all()
