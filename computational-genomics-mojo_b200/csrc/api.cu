@@ -86,7 +86,7 @@ void exec_free(Exec &x)
             cudaStreamSynchronize(x.aux[i]);
     DevBuf *bufs[] = {&x.keys,      &x.queue,     &x.counts, &x.seg,   &x.counters,
                       &x.scratch64, &x.scratch32, &x.work,   &x.errflag, &x.tierq,
-                      &x.dumps};
+                      &x.dumps,     &x.ubound};
     for (DevBuf *b : bufs)
         if (b->p) {
             cudaFree(b->p);
@@ -635,7 +635,7 @@ static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
 // launches after the first take their pair count from the device.  With
 // GB2_FLAG_BATCHED the first tier's queue is ordered longest first.
 static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
-                     const WfaParams &p, int64_t n, int32_t *d_out, int flags)
+                     const WfaParams &p, int64_t n, int32_t *d_out, int flags, int32_t *d_ub)
 {
     const WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
     const int64_t sms = c->sm_count;
@@ -724,6 +724,8 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
             io.restart_n = q_n + kCounterStride * 2;
         }
         io.gring = (int32_t *)x.scratch32.p;
+        // the tiers after S prune by the bound pass's costs
+        io.ubound = (d_ub && t > 0) ? d_ub : nullptr;
         const int64_t per = teams_per_block[t];
         const int grid = (int)(t == first ? std::min<int64_t>(sms, (n + per - 1) / per) : sms);
         cudaEvent_t e0 = prof_begin(c, x.st);
@@ -731,6 +733,27 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
                               (int *)x.errflag.p, x.st));
         prof_end(c, e0, x.st);
         c->launches += 1;
+        if (t == 0 && d_ub && nt >= 0) {
+            // The bound pass: the pairs S suspended continue from their records
+            // (read, not consumed) on the S kernel inside a band of
+            // +-kWfaBoundBand diagonals around the line from diagonal 0 to the
+            // target.  A hit there is a real alignment, so its cost bounds the
+            // optimum from above; a pair the band cannot finish gets -1 (the
+            // bound is then max_error).
+            WfaTierIo bp{};
+            bp.ctr = in_ctr + kCounterStride * 10;
+            bp.ents = io.next;
+            bp.n_dev = io.next_n;
+            bp.dumps_in = io.dumps_out;
+            bp.dump_in_stride = io.dump_out_stride;
+            bp.band_w = kWfaBoundBand;
+            bp.gring = io.gring;
+            cudaEvent_t e1 = prof_begin(c, x.st);
+            CU(c, launch_wfa_tier(pl, 0, (int)sms, qv, rv, p, bp, d_ub, (int64_t *)x.work.p,
+                                  (int *)x.errflag.p, x.st));
+            prof_end(c, e1, x.st);
+            c->launches += 1;
+        }
         prev = t;
     }
     return GB2_OK;
@@ -746,8 +769,22 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     const WfaParams p{cfg->x, cfg->o, cfg->e, cfg->max_error};
     // the tiered kernels, unless the call asks for the naive baseline, a tuning
     // variant of the single-kernel design below, or the CIGAR pass's history sizes
-    if (!(flags & GB2_FLAG_NAIVE) && ((flags >> 8) & 0xff) == 0 && !d_hist)
-        return wfa_tiers(c, x, qv, rv, qmax, rmax, p, n, d_out, flags);
+    if (!(flags & GB2_FLAG_NAIVE) && ((flags >> 8) & 0xff) == 0 && !d_hist) {
+        // Batches with long pairs: for every pair the S tier suspends (the
+        // expensive ones), a bound pass finds the cost of its best alignment
+        // inside a band of +-kWfaBoundBand diagonals around the line from
+        // diagonal 0 to the target -- the cost of a real alignment, so no lower
+        // than the optimum -- and the later tiers skip every diagonal that cannot
+        // finish within it (s + e*|k - target| > bound): the same costs, far
+        // fewer cells where the wavefronts are widest.
+        if ((flags & GB2_FLAG_NO_PRUNE) || std::max(qmax, rmax) < kWfaBoundMinLen)
+            return wfa_tiers(c, x, qv, rv, qmax, rmax, p, n, d_out, flags, nullptr);
+        int rc;
+        if ((rc = ensure(c, x.ubound, (size_t)n * 4, x.st)))
+            return rc;
+        CU(c, cudaMemsetAsync(x.ubound.p, 0xff, (size_t)n * 4, x.st));  // -1: no bound yet
+        return wfa_tiers(c, x, qv, rv, qmax, rmax, p, n, d_out, flags, (int32_t *)x.ubound.p);
+    }
     const int g = gcd_h(cfg->x, gcd_h(cfg->o, cfg->e));
     const int hm = std::max(cfg->x / g, (cfg->o + cfg->e) / g) + 1, hie = cfg->e / g + 1;
     const int nslot = hm + 2 * hie;

@@ -147,6 +147,11 @@ struct WfaTierIo {
     int2 *restart;
     int *restart_n;
     int32_t *gring;  // G tier: grid regions of gring_block_bytes
+    // exact pruning: per pair a cost no lower than the optimum (-1: max_error), so
+    // diagonals k with s + e*|k - target| above it are skipped; and the bound
+    // pass's band half-width (> 0: only [min(0, target) - w, max(0, target) + w])
+    const int32_t *ubound;
+    int32_t band_w;
 };
 cudaError_t launch_wfa_tier(const WfaTierPlan &pl, int tier, int grid, SeqView q, SeqView r,
                             WfaParams p, const WfaTierIo &io, int32_t *out, int64_t *work,

@@ -28,6 +28,10 @@ constexpr int64_t kWideHmax = 4094;
 constexpr int64_t kWfaScratchCap = 8ll << 30;  // WFA rings of all warps, bytes
 constexpr int64_t kWfaTeamMinLen = 2048;       // shortest WFA pair aligned by a whole block
 constexpr int64_t kTierDumpCap = 1ll << 30;    // bytes of suspended-pair records per transition
+// WFA bound pass: batches whose longest sequence has at least kWfaBoundMinLen
+// bases run it, over a band of +-kWfaBoundBand diagonals
+constexpr int64_t kWfaBoundMinLen = 1024;
+constexpr int32_t kWfaBoundBand = 64;
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -47,6 +51,7 @@ struct Exec {
     cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
     DevBuf keys, queue, counts, seg, counters, scratch64, scratch32, work, errflag;
     DevBuf tierq, dumps;  // tiered WFA: the M/L/G queues and the suspended pairs' records
+    DevBuf ubound;        // WFA: per pair, the bound pass's cost (an upper bound of the optimum)
 };
 
 // Device buffers of the WFA CIGAR entry point (grow-only, per context).

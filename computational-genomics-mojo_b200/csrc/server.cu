@@ -185,7 +185,7 @@ int64_t group_bytes(const Layout &l, const gb2_wfa_cfg &w, int sm_count)
         // transitions, and the G tier's per-block rings
         const WfaTierPlan pl = wfa_tier_plan(WfaParams{w.x, w.o, w.e, w.max_error},
                                              l.wfa_qmax, l.wfa_rmax);
-        int64_t tiers = l.n_wfa * 24 + (int64_t)sm_count * pl.gring_block_bytes;
+        int64_t tiers = l.n_wfa * 28 + (int64_t)sm_count * pl.gring_block_bytes;
         for (int t = 0; t < 2; ++t)
             tiers += std::min<int64_t>(l.n_wfa, kTierDumpCap / pl.dump_stride[t]) *
                      pl.dump_stride[t];
@@ -483,7 +483,8 @@ int gb2_server_start(gb2_ctx *c, const gb2_server_cfg *cfg, gb2_server **out)
         auto sl = std::make_unique<Slot>();
         for (DevBuf *b : {&sl->d_in, &sl->d_out, &sl->x.keys, &sl->x.queue, &sl->x.counts,
                           &sl->x.seg, &sl->x.counters, &sl->x.scratch64, &sl->x.scratch32,
-                          &sl->x.work, &sl->x.errflag, &sl->x.tierq, &sl->x.dumps})
+                          &sl->x.work, &sl->x.errflag, &sl->x.tierq, &sl->x.dumps,
+                          &sl->x.ubound})
             b->pool = s->pool;
         if (exec_init(sl->x) != GB2_OK) {
             exec_free(sl->x);

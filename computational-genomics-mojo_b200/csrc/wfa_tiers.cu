@@ -174,7 +174,7 @@ __device__ __forceinline__ SeqWin stage_seq(const SeqView &v, int64_t off, int32
 // 16-base windows, leading zeros / 2 = matching bases, clamped by the
 // remaining lengths.  Requires row >= 0 and row - k >= 0.
 template <bool SMEM>
-__device__ __forceinline__ int32_t ext_run(const SeqWin &qs, int32_t qlen, const SeqWin &rs,
+__device__ __noinline__ int32_t ext_run(const SeqWin &qs, int32_t qlen, const SeqWin &rs,
                                            int32_t rlen, int32_t row, int32_t k)
 {
     int32_t col = row - k;
@@ -248,7 +248,7 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                                              const Team<TEAM, NTEAMS> &team,
                                              volatile int64_t *bcast, const uint8_t *resume,
                                              const DumpOut &dump, int64_t *dump_idx,
-                                             int64_t &cells)
+                                             int64_t &cells, int32_t band_w, int32_t ub)
 {
     constexpr int TW = TEAM * 32;
     constexpr int32_t NEG = Neg<RT>::value;
@@ -269,7 +269,7 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
     const SeqWin rs = stage_seq<SMEM_SEQ>(r, roff, rnw, sr, tt, TW);
     // every ring element NEG
     {
-        const int32_t total = w.nslot * W;
+        const int32_t total = (w.nslot + 1) * W;  // the slots and the NEG row
         if (R16) {
             // W is a multiple of 8 and the window 16-byte aligned
             uint4 *v = reinterpret_cast<uint4 *>(ring);
@@ -339,6 +339,22 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
             }
             lo = max(lo, -max_err);
             hi = min(hi, max_err);
+            if (band_w > 0) {
+                // the bound pass: only the band around the line from diagonal 0 to
+                // the target, which still holds real alignments (their costs bound
+                // the optimum from above)
+                lo = max(lo, min(0, target) - band_w);
+                hi = min(hi, max(0, target) + band_w);
+            }
+            if (ub >= 0) {
+                // a diagonal k at score s costs at least s + e*|k - target| to finish
+                // (every diagonal change is a gap base): beyond the upper bound ub it
+                // cannot be on an alignment of cost <= ub, and dropping it only
+                // lowers values elsewhere, so the first hit stays at the same s
+                const int32_t R = (ub - s) / p.e;
+                lo = max(lo, target - R);
+                hi = min(hi, target + R);
+            }
             const int sx = sp >= xs ? (nms >= xs ? nms - xs : nms - xs + hm) : -1;
             const int soe = sp >= oes ? (nms >= oes ? nms - oes : nms - oes + hm) : -1;
             const int se = sp >= es ? (nis >= es ? nis - es : nis - es + hie) : -1;
@@ -450,10 +466,12 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
             bool hit = false;
             if (a <= b) {
                 cells += (int64_t)(b - a + 1);
-                const RT *Mx = sx >= 0 ? slot(sx) : nullptr;
-                const RT *Moe = soe >= 0 ? slot(soe) : nullptr;
-                const RT *Ie = se >= 0 ? slot(hm + se) : nullptr;
-                const RT *De = se >= 0 ? slot(hm + hie + se) : nullptr;
+                // a source that does not exist yet reads the row kept NEG (slot nslot)
+                const RT *negrow = slot(w.nslot);
+                const RT *Mx = sx >= 0 ? slot(sx) : negrow;
+                const RT *Moe = soe >= 0 ? slot(soe) : negrow;
+                const RT *Ie = se >= 0 ? slot(hm + se) : negrow;
+                const RT *De = se >= 0 ? slot(hm + hie + se) : negrow;
                 // rounds of UU diagonals per thread: full rounds (every diagonal
                 // inside [a, b]) while they last, then single-diagonal rounds
                 auto round = [&](int32_t k0, auto uc, auto fc) {
@@ -466,17 +484,9 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                         ks[u] = k0 + TW * u;
                         live[u] = FULLR || ks[u] <= b;
                         const int32_t kc = FULLR ? ks[u] : (live[u] ? ks[u] : b);
-                        int32_t io = NEG, ie = NEG, dop = NEG, dex = NEG, mx = NEG;
-                        if (Moe) {
-                            io = (int32_t)Moe[kc - 1];
-                            dop = (int32_t)Moe[kc + 1];
-                        }
-                        if (Ie) {
-                            ie = (int32_t)Ie[kc - 1];
-                            dex = (int32_t)De[kc + 1];
-                        }
-                        if (Mx)
-                            mx = (int32_t)Mx[kc];
+                        const int32_t io = (int32_t)Moe[kc - 1], dop = (int32_t)Moe[kc + 1];
+                        const int32_t ie = (int32_t)Ie[kc - 1], dex = (int32_t)De[kc + 1];
+                        const int32_t mx = (int32_t)Mx[kc];
                         const int32_t i0 = max(io, ie), d0 = max(dop, dex);
                         // max(mx + 1, i0 + 1, d0) as two DPX add-max instructions
                         const int32_t m1 = __viaddmax_s32(mx, 1, __viaddmax_s32(i0, 1, d0));
@@ -541,6 +551,8 @@ struct TierIn {
     int *ctr;
     const uint8_t *dumps;   // records the entries refer to
     int64_t dump_stride;
+    const int32_t *ubound;  // per pair: a cost no lower than the optimum (-1: max_error)
+    int32_t band_w;         // > 0: the bound pass's band half-width
 };
 
 struct TierOut {
@@ -574,7 +586,7 @@ wfa_tier_kernel(SeqView q, SeqView r, WfaParams p, TierIn in, TierOut tout, Tier
     RT *ring;
     if (GRING)
         ring = reinterpret_cast<RT *>(geo.gring +
-                                      (int64_t)blockIdx.x * w.nslot * (int64_t)geo.W);
+                                      (int64_t)blockIdx.x * (w.nslot + 1) * (int64_t)geo.W);
     else
         ring = reinterpret_cast<RT *>(mine);
     uint2 *const sq = reinterpret_cast<uint2 *>(mine + geo.ring_bytes);
@@ -612,12 +624,20 @@ wfa_tier_kernel(SeqView q, SeqView r, WfaParams p, TierIn in, TierOut tout, Tier
                               2 * ((rl + 31) >> 5) <= geo.seq_cap;
         int64_t di = -2;
         int32_t res;
+        int32_t ub = -1;
+        if (in.ubound) {
+            ub = in.ubound[pi];
+            if (ub < 0)
+                ub = p.max_error;
+        }
         if (smem_seq)
             res = tier_pair<TEAM, NTEAMS, 4, true, RT>(q, r, p, w, pi, ring, geo.W, geo.H, sq, sr,
-                                                       team, bc, resume, tout.dump, &di, cells);
+                                                       team, bc, resume, tout.dump, &di, cells,
+                                                       in.band_w, ub);
         else
             res = tier_pair<TEAM, NTEAMS, 4, false, RT>(q, r, p, w, pi, ring, geo.W, geo.H, sq, sr,
-                                                        team, bc, resume, tout.dump, &di, cells);
+                                                        team, bc, resume, tout.dump, &di, cells,
+                                                        in.band_w, ub);
         if (tt == 0) {
             if (res >= -1) {
                 out[pi] = res;
@@ -628,6 +648,8 @@ wfa_tier_kernel(SeqView q, SeqView r, WfaParams p, TierIn in, TierOut tout, Tier
                 // kRestart, or a window overflow with no tier above: the G tier
                 const int slot = atomicAdd(tout.restart_n, 1);
                 tout.restart[slot] = make_int2((int)pi, -1);
+            } else if (in.band_w > 0) {
+                out[pi] = -1;  // the bound pass could not finish this pair: no bound
             } else {
                 out[pi] = -3;  // no tier left (the G window holds every diagonal)
                 atomicOr(err_flag, 1);
@@ -672,13 +694,13 @@ WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
         const int64_t team_bytes = kTierBlockSmem / s.nteams;
         const int64_t seq_entries = 2 * ((s.seq_bases + 31) / 32);  // halves per sequence
         const int64_t seq_bytes = 2 * seq_entries * 8;
-        int64_t W = (team_bytes - seq_bytes) / (nslot * 2);
+        int64_t W = (team_bytes - seq_bytes) / ((nslot + 1) * 2);
         W = W / 8 * 8;  // 16-byte rows: the NEG fill uses 16-byte stores
         plan.W[t] = (int32_t)W;
         plan.H[t] = (int32_t)(W / 2 - 1);
         plan.seq_cap[t] = (int32_t)seq_entries;
         plan.team_bytes[t] = team_bytes & ~int64_t(15);
-        plan.ring_bytes[t] = (int64_t)nslot * W * 2;
+        plan.ring_bytes[t] = (int64_t)(nslot + 1) * W * 2;
         plan.usable[t] = W >= 64;
         plan.dump_stride[t] = (kDumpHeader + (int64_t)nslot * W * 2 + 255) & ~int64_t(255);
     }
@@ -690,7 +712,7 @@ WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
     plan.team_bytes[3] = 2 * (int64_t)plan.seq_cap[3] * 8;
     plan.ring_bytes[3] = 0;
     plan.usable[3] = true;
-    plan.gring_block_bytes = (int64_t)nslot * plan.W[3] * 4;
+    plan.gring_block_bytes = (int64_t)(nslot + 1) * plan.W[3] * 4;
     return plan;
 }
 
@@ -716,7 +738,8 @@ cudaError_t launch_wfa_tier(const WfaTierPlan &pl, int tier, int grid, SeqView q
                             WfaParams p, const WfaTierIo &io, int32_t *out, int64_t *work,
                             int *err_flag, cudaStream_t st)
 {
-    TierIn in{io.list, io.ents, io.n, io.n_dev, io.seg, io.ctr, io.dumps_in, io.dump_in_stride};
+    TierIn in{io.list,    io.ents,           io.n,      io.n_dev, io.seg,
+              io.ctr,     io.dumps_in,       io.dump_in_stride,   io.ubound, io.band_w};
     TierOut o{io.next, io.next_n, DumpOut{io.dumps_out, io.dump_out_stride, io.dump_out_cap,
                                           io.dump_out_ctr},
               io.restart, io.restart_n};

@@ -35,6 +35,7 @@ FLAG_INT32 = 0x2
 FLAG_GENERIC = 0x4
 FLAG_GRAPH = 0x8  # capture resident calls into a CUDA graph and replay it
 FLAG_NAIVE = 0x10  # baseline: one thread block per pair, input order, no planning
+FLAG_NO_PRUNE = 0x20  # WFA: no bound pass, every reachable diagonal (same results)
 
 
 class SwCfg(ctypes.Structure):

@@ -85,6 +85,9 @@ typedef struct gb2_batch gb2_batch;
                                   path is measured against -- one launch, one thread block
                                   per pair in input order, no planning, as the reference's
                                   launchers do (genomics/gpu/align_gpu.mojo:482-492, :524-534) */
+#define GB2_FLAG_NO_PRUNE 0x20 /* gb2_wfa_affine: skip the bound pass (a banded WFA whose
+                                  costs bound the optimum from above) and the exact pass's
+                                  pruning by it; results are the same either way */
 /* Tuning fields (0 = the library's choice): bits 8-15 select a kernel
  * variant; bits 16-23 set how many chunks the *_host entry points split a
  * batch into for their copy/compute pipeline. */

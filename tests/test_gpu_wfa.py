@@ -198,3 +198,19 @@ def test_int16_step_cap_rerun(device, oracle):
     assert (ref >= 0).all() and (ref // 2 > 32767 - 31800).any()
     for batched in (True, False):
         assert_same(device.wfa_affine(q, r, cfg, batched=batched), ref, f"batched={batched}")
+
+
+def test_bound_pruning_gives_the_same_costs(device, oracle):
+    """Batches with long pairs run a bound pass (a banded WFA over the pairs the
+    first tier suspends) and prune the later tiers by it; GB2_FLAG_NO_PRUNE turns
+    both off.  Both equal the oracle, at the exact-cover budget and at budgets
+    below some pairs' costs (-1), with penalty sets of other slot counts."""
+    from genomics_b200._lib import FLAG_NO_PRUNE
+    q, r, _, _ = synth.generate(2, 4000, seed=77)
+    for pen in ((4, 6, 2), (2, 3, 1), (5, 2, 3)):
+        for me in (synth.wfa_max_error_cover(q, r, *pen), 1500):
+            cfg = WFAConfig(*pen, me)
+            ref = oracle_wfa(oracle, q, r, cfg)
+            for fl in (0, FLAG_NO_PRUNE):
+                assert_same(device.wfa_affine(q, r, cfg, batched=True, flags=fl), ref,
+                            f"{pen} me={me} flags={fl}")
