@@ -255,6 +255,18 @@ def wfa_parity(q, r, got, cfg, threads):
     return f"{int((want == got).sum())}/{want.size}"
 
 
+def workload_config(args, cells, seed):
+    """The `config` object of both arms' lines: the same workload, named by its sizes."""
+    from genomics_b200 import synth
+    return {"workload": WORKLOAD, "pairs_per_gpu": args.pairs, "band": BAND,
+            "query_bp": 150, "target_bp": 200, "scoring": list(SCORING),
+            "path": "plain" if args.plain else "batched", "variant": args.variant,
+            "l2": "flushed between timed steps (256 MB device write)",
+            "cells_per_step_per_gpu": int(cells),
+            "generator": synth.GENERATOR, "seed": hex(seed),
+            "seed_rule": "0xb2000001 + 7919 * rank"}
+
+
 def reference_arm(args, dist: Dist):
     """The reference's CPU algorithm, timed on this host's cores."""
     if dist.rank != 0:
@@ -270,12 +282,12 @@ def reference_arm(args, dist: Dist):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "pairs_per_step": sample,
-                   "note": "reference is Mojo-only (no toolchain here); its CPU algorithm "
-                           "runs as the C restatement in oracle/"},
+        "config": workload_config(args, synth.sw_cells(q, BAND), synth.default_seed(1)),
+        "note": "the reference is Mojo-only (no toolchain here); its CPU algorithm runs as "
+                "the C restatement in oracle/, each step a bounded sample of the workload",
         "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads,
                          "kind": "port",
-                         "sample": f"{sample} of the {args.pairs} pairs per step"},
+                         "sample": f"first {sample} of the {args.pairs} pairs per step"},
         "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -402,13 +414,7 @@ def our_arm(args, dist: Dist):
             "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "int16x2" if packed else "int32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_gpu": args.pairs, "band": BAND,
-                       "query_bp": 150, "target_bp": 200, "scoring": list(SCORING),
-                       "path": "batched" if batched else "plain", "variant": args.variant,
-                       "l2": "flushed between timed steps (256 MB device write)",
-                       "cells_per_step_per_gpu": cells,
-                       "generator": synth.GENERATOR, "seed": hex(seed),
-                       "seed_rule": "0xb2000001 + 7919 * rank"},
+            "config": workload_config(args, cells, seed),
             "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GCUPS",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,

@@ -199,26 +199,34 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
                                       int32_t rlen, int32_t (&rows)[U], const int32_t (&ks)[U],
                                       const bool (&live)[U])
 {
-    uint32_t x[U];
-    int32_t lim[U];
-    bool go[U];
+    // Either sequence empty: no diagonal can extend (and there is no window to load).
+    if (qlen <= 0 || rlen <= 0)
+        return;
+    // Live rows are >= 0 (and so are their columns); dead rows are negative and
+    // must not move.  Window positions are clamped into the sequences, so every
+    // load is in bounds, and the advance max(0, min(ml, qlen - row, rlen - col))
+    // is zeroed for dead rows and for diagonals past the last one.
+    int32_t adv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int32_t row = rows[u], col = row - ks[u];
-        go[u] = live[u] && (uint32_t)row < (uint32_t)qlen && (uint32_t)col < (uint32_t)rlen;
-        lim[u] = min(qlen - row, rlen - col);
-        x[u] = 0;
-        if (go[u])
-            x[u] = win16<SMEM>(qs, row) ^ win16<SMEM>(rs, col);
+        const int32_t pq = (int32_t)min((uint32_t)row, (uint32_t)(qlen - 1));
+        const int32_t pr = (int32_t)min((uint32_t)col, (uint32_t)(rlen - 1));
+        const uint32_t x = win16<SMEM>(qs, pq) ^ win16<SMEM>(rs, pr);
+        const int32_t ml = __clz((int)x) >> 1;
+        int32_t a = __vimin3_s32_relu(ml, qlen - row, rlen - col);
+        a &= ~(row >> 31);
+        if (!live[u])
+            a = 0;
+        adv[u] = a;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        if (!go[u])
-            continue;
-        const int ml = __clz((int)x[u]) >> 1;
-        rows[u] += min(ml, lim[u]);
-        if (ml == 16 && lim[u] > 16)
-            rows[u] = ext_run<SMEM>(qs, qlen, rs, rlen, rows[u], ks[u]);
+        const int32_t row = rows[u] + adv[u];
+        rows[u] = row;
+        // a whole window matched and both sequences go on: the rest one by one
+        if (adv[u] == 16 && row < qlen && row - ks[u] < rlen)
+            rows[u] = ext_run<SMEM>(qs, qlen, rs, rlen, row, ks[u]);
     }
 }
 
