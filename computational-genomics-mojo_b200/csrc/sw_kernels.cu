@@ -286,12 +286,16 @@ sw_band_kernel(SeqView q, SeqView r, SwParams p, PairList pl, gb2_sw_result *__r
 // kernel arguments rather than literals so that the multiply-adds using them
 // stay multiply-adds.
 struct Pack16Consts {
-    uint32_t one, x4, x8, x32, x128, x256, half;
+    uint32_t one, x4, x128, x256, half;
     uint32_t dm[4];  // (match - mismatch) << 18, 20, 22, 24
     uint32_t mmg2;   // mismatch - (go+ge) in both halves
     uint32_t neg_g2; // minus -(go+ge) in both halves, mod 2^32
     uint32_t ge2;    // ge in both halves
     uint32_t ng2;    // -(go+ge) in both halves
+    // the wide-key multipliers stay last: with them placed before x128 the narrow
+    // band-32 kernel measured 9% slower (665 vs 610 us per 262,144-pair launch,
+    // same registers)
+    uint32_t x8, x32;
 };
 
 __device__ __forceinline__ uint32_t mad_hi_u32(uint32_t a, uint32_t b, uint32_t c)

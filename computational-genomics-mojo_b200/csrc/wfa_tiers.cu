@@ -331,6 +331,12 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
             result = 0;
     }
     team.sync();
+    int32_t rq = 0, rr = 0;  // pruning: (ub - s) / e and its remainder at s = sp0 * g
+    if (ub >= 0) {
+        const int32_t num = ub - (int32_t)(sp0 * g);
+        rq = num / p.e;
+        rr = num - rq * p.e;
+    }
     if (result == kRunning) {
         for (int64_t sp = sp0; sp * g <= max_err; ++sp) {
             if (R16 && sp > 32767 - (int64_t)qlen) {
@@ -359,7 +365,14 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                 // (every diagonal change is a gap base): beyond the upper bound ub it
                 // cannot be on an alignment of cost <= ub, and dropping it only
                 // lowers values elsewhere, so the first hit stays at the same s
-                const int32_t R = (ub - s) / p.e;
+                // R = (ub - s) / e, kept as quotient and remainder (s grows by g
+                // per step, and ub >= s while the pair runs)
+                const int32_t R = rq;
+                rr -= g;
+                if (rr < 0) {
+                    rr += p.e;
+                    --rq;
+                }
                 lo = max(lo, target - R);
                 hi = min(hi, target + R);
             }
