@@ -213,7 +213,8 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
         const int32_t pq = (int32_t)min((uint32_t)row, (uint32_t)(qlen - 1));
         const int32_t pr = (int32_t)min((uint32_t)col, (uint32_t)(rlen - 1));
         const uint32_t x = win16<SMEM>(qs, pq) ^ win16<SMEM>(rs, pr);
-        const int32_t ml = __clz((int)x) >> 1;
+        int32_t ml = __clz((int)x) >> 1;
+        ml += ml >> 4;  // 17 for a whole matching window
         int32_t a = __vimin3_s32_relu(ml, qlen - row, rlen - col);
         a &= ~(row >> 31);
         if (!live[u])
@@ -222,11 +223,11 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int32_t row = rows[u] + adv[u];
-        rows[u] = row;
-        // a whole window matched and both sequences go on: the rest one by one
-        if (adv[u] == 16 && row < qlen && row - ks[u] < rlen)
-            rows[u] = ext_run<SMEM>(qs, qlen, rs, rlen, row, ks[u]);
+        // 17: the window matched and both sequences go on past it: the rest one by one
+        if (adv[u] == 17)
+            rows[u] = ext_run<SMEM>(qs, qlen, rs, rlen, rows[u] + 16, ks[u]);
+        else
+            rows[u] += adv[u];
     }
 }
 
@@ -338,11 +339,11 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
         rr = num - rq * p.e;
     }
     if (result == kRunning) {
-        for (int64_t sp = sp0; sp * g <= max_err; ++sp) {
-            if (R16 && sp > 32767 - (int64_t)qlen) {
-                result = kRestart;  // past the steps int16 values are proven for
-                break;
-            }
+        // steps s = sp * g <= max_err; int16 rows are proven for sp <= 32767 - qlen
+        const int32_t sp_end = max_err / g;
+        const int32_t sp_lim = R16 ? min(sp_end, 32767 - qlen) : sp_end;
+        int32_t sp = (int32_t)sp0;
+        for (; sp <= sp_lim; ++sp) {
             const int32_t s = (int32_t)(sp * g);
             const int nms = ms + 1 == hm ? 0 : ms + 1;
             const int nis = is + 1 == hie ? 0 : is + 1;
@@ -536,7 +537,7 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                 for (; k0 <= b; k0 += TW)
                     round(k0, std::integral_constant<int, 1>{}, std::false_type{});
                 // the thread that owns the target diagonal reads back its own store
-                if (target >= a && target <= b && ((target - a) % TW) == tt)
+                if ((uint32_t)(target - a) <= (uint32_t)(b - a) && ((target - a) & (TW - 1)) == tt)
                     hit = (int32_t)Mw[target] >= qlen;
             }
             if (lane == ms) {
@@ -554,7 +555,8 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
             }
         }
         if (result == kRunning)
-            result = -1;  // the loop ran out: cost above max_error (:226)
+            result = sp <= sp_end ? kRestart  // past the steps int16 values are proven for
+                                  : -1;       // the loop ran out: cost above max_error (:226)
     }
     return result;
 }
