@@ -423,8 +423,12 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
     return rk;
 }
 
+// Band 128 is register-bound to two blocks per SM either way; with the
+// minimum-blocks hint of 1 the compiler schedules it in 254 registers instead
+// of 251 and the kernel measured 6% faster (2,734 vs 2,583 GCUPS).  The other
+// widths keep the default schedule (hint 0).
 template <int B, bool WIDE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, (B == 128) ? 1 : 0)
 sw_pack16_kernel(SeqView q, SeqView r, Pack16Consts c, PairList pl, gb2_sw_result *__restrict__ out)
 {
     static_assert(B % 16 == 0, "band must be a multiple of 16");
