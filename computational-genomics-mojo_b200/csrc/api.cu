@@ -628,9 +628,9 @@ static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
 
 // Tiered WFA (wfa_tiers.cu): every pair starts on the smallest team whose
 // launch still fills the GPU -- one warp (S) for large batches, four warps (M)
-// for up to 16 pairs per SM, sixteen (L) for up to two per SM, so a single long
-// pair (the per-call drop-in) gets a whole SM -- and moves up a tier when its
-// wavefront outgrows the window; pairs that outgrow L or need int32 rows
+// for up to 16 pairs per SM, eight (L) for up to two per SM, sixteen (XL) for
+// one, so a single long pair (the per-call drop-in) gets a whole SM -- and moves
+// up a tier when its wavefront outgrows the window; pairs that outgrow XL or need int32 rows
 // finish in G.  One launch per tier from the first, in order on x.st; the
 // launches after the first take their pair count from the device.  With
 // GB2_FLAG_BATCHED the first tier's queue is ordered longest first.
@@ -639,18 +639,19 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
 {
     const WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
     const int64_t sms = c->sm_count;
-    int first = n <= 2 * sms ? 2 : (n <= 16 * sms ? 1 : 0);
-    while (first < 3 && !pl.usable[first])
+    constexpr int G = kWfaShared;  // the global-memory tier
+    int first = n <= sms ? 3 : (n <= 2 * sms ? 2 : (n <= 16 * sms ? 1 : 0));
+    while (first < G && !pl.usable[first])
         ++first;
     auto next_of = [&](int t) {
-        for (int u = t + 1; u < 3; ++u)
+        for (int u = t + 1; u < G; ++u)
             if (pl.usable[u])
                 return u;
         return -1;
     };
     // dump records of the transitions out of the first two tiers
-    int64_t dcap[3] = {0, 0, 0}, doff[3] = {0, 0, 0}, dbytes = 0;
-    for (int t = first; t < 3; ++t) {
+    int64_t dcap[G] = {}, doff[G] = {}, dbytes = 0;
+    for (int t = first; t < G; ++t) {
         if (!pl.usable[t] || next_of(t) < 0)
             continue;
         dcap[t] = std::min<int64_t>(n, kTierDumpCap / pl.dump_stride[t]);
@@ -658,16 +659,18 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
         dbytes += dcap[t] * pl.dump_stride[t];
     }
     int rc;
-    if ((rc = ensure(c, x.tierq, (size_t)n * 24, x.st)) ||
+    if ((rc = ensure(c, x.tierq, (size_t)n * 8 * G, x.st)) ||
         (rc = ensure(c, x.dumps, (size_t)std::max<int64_t>(dbytes, 256), x.st)) ||
         (rc = ensure(c, x.scratch32, (size_t)(sms * pl.gring_block_bytes), x.st)) ||
         (rc = ensure(c, x.counters, kCounterBytes, x.st)))
         return rc;
     CU(c, cudaMemsetAsync(x.counters.p, 0, kCounterBytes, x.st));
     int *const ctr = (int *)x.counters.p;
-    int *const in_ctr = ctr;                         // + 32 * tier
-    int *const q_n = ctr + 4 * kCounterStride;       // + 32 * (tier - 1): pairs queued for M, L, G
-    int *const d_ctr = ctr + 7 * kCounterStride;     // + 32 * tier: records claimed
+    int *const in_ctr = ctr;                             // + 32 * tier
+    int *const q_n = ctr + (G + 1) * kCounterStride;     // + 32 * (tier - 1): pairs queued for tiers 1..G
+    int *const d_ctr = ctr + (2 * G + 1) * kCounterStride;  // + 32 * tier: records claimed
+    int *const b_ctr = ctr + (3 * G + 1) * kCounterStride;  // the bound pass
+    static_assert((3 * G + 2) * kCounterStride * 4 <= (int)kCounterBytes, "counter space");
     int2 *const tq = (int2 *)x.tierq.p;              // + n * (tier - 1)
     uint8_t *const dumps = (uint8_t *)x.dumps.p;
     const int32_t *list = nullptr;
@@ -691,10 +694,10 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
         list = (const int32_t *)x.queue.p;
         seg = (const int64_t *)x.seg.p;
     }
-    static const int teams_per_block[4] = {16, 4, 1, 1};
+    static const int teams_per_block[G + 1] = {16, 4, 2, 1, 1};
     int prev = -1;  // the tier launched before t: its suspended pairs are t's entries
-    for (int t = first; t < 4; ++t) {
-        if (t < 3 && !pl.usable[t])
+    for (int t = first; t <= G; ++t) {
+        if (t < G && !pl.usable[t])
             continue;
         WfaTierIo io{};
         io.ctr = in_ctr + kCounterStride * t;
@@ -705,12 +708,12 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
         } else {
             io.ents = tq + n * (t - 1);
             io.n_dev = q_n + kCounterStride * (t - 1);
-            if (t < 3 && prev >= 0 && dcap[prev] > 0) {  // G entries always start over
+            if (t < G && prev >= 0 && dcap[prev] > 0) {  // G entries always start over
                 io.dumps_in = dumps + doff[prev];
                 io.dump_in_stride = pl.dump_stride[prev];
             }
         }
-        const int nt = t < 3 ? next_of(t) : -1;
+        const int nt = t < G ? next_of(t) : -1;
         if (nt >= 0) {
             io.next = tq + n * (nt - 1);
             io.next_n = q_n + kCounterStride * (nt - 1);
@@ -719,9 +722,9 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
             io.dump_out_cap = dcap[t];
             io.dump_out_ctr = d_ctr + kCounterStride * t;
         }
-        if (t < 3) {
-            io.restart = tq + n * 2;
-            io.restart_n = q_n + kCounterStride * 2;
+        if (t < G) {
+            io.restart = tq + n * (G - 1);
+            io.restart_n = q_n + kCounterStride * (G - 1);
         }
         io.gring = (int32_t *)x.scratch32.p;
         // the tiers after S prune by the bound pass's costs
@@ -741,7 +744,7 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
             // optimum from above; a pair the band cannot finish gets -1 (the
             // bound is then max_error).
             WfaTierIo bp{};
-            bp.ctr = in_ctr + kCounterStride * 10;
+            bp.ctr = b_ctr;
             bp.ents = io.next;
             bp.n_dev = io.next_n;
             bp.dumps_in = io.dumps_out;

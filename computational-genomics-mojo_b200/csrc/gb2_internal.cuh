@@ -110,16 +110,18 @@ cudaError_t launch_wfa(int variant, int block_warps, SeqView q, SeqView r, WfaPa
                        cudaStream_t st);
 
 // Tiered WFA (wfa_tiers.cu): tier 0 (S) one warp per pair, 1 (M) four warps,
-// 2 (L) sixteen warps, rings of W int16 per slot in shared memory; tier 3 (G)
-// sixteen warps, int32 rings in global memory covering every diagonal.
+// 2 (L) eight warps, 3 (XL) sixteen warps, rings of W int16 per slot in shared
+// memory; tier kWfaShared (G) sixteen warps, int32 rings in global memory
+// covering every diagonal.
+constexpr int kWfaShared = 4;  // tiers with their rings in shared memory
 struct WfaTierPlan {
     int nslot;
-    int32_t W[4], H[4];        // window per slot row; element of diagonal 0
-    int32_t seq_cap[4];        // 16-base window entries of a sequence copy
-    int64_t team_bytes[4];     // shared bytes per team
-    int64_t ring_bytes[4];     // of them, the ring
-    int64_t dump_stride[3];    // bytes of a suspended pair's record, per source tier
-    bool usable[4];            // the window holds at least 64 diagonals
+    int32_t W[kWfaShared + 1], H[kWfaShared + 1];  // window per slot row; element of diagonal 0
+    int32_t seq_cap[kWfaShared + 1];     // 16-base window entries of a sequence copy
+    int64_t team_bytes[kWfaShared + 1];  // shared bytes per team
+    int64_t ring_bytes[kWfaShared + 1];  // of them, the ring
+    int64_t dump_stride[kWfaShared];     // bytes of a suspended pair's record, per source tier
+    bool usable[kWfaShared + 1];         // the window holds at least 64 diagonals
     int64_t gring_block_bytes; // G tier ring region of one block
 };
 WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax);

@@ -185,8 +185,8 @@ int64_t group_bytes(const Layout &l, const gb2_wfa_cfg &w, int sm_count)
         // transitions, and the G tier's per-block rings
         const WfaTierPlan pl = wfa_tier_plan(WfaParams{w.x, w.o, w.e, w.max_error},
                                              l.wfa_qmax, l.wfa_rmax);
-        int64_t tiers = l.n_wfa * 28 + (int64_t)sm_count * pl.gring_block_bytes;
-        for (int t = 0; t < 2; ++t)
+        int64_t tiers = l.n_wfa * (8 * kWfaShared + 4) + (int64_t)sm_count * pl.gring_block_bytes;
+        for (int t = 0; t + 1 < kWfaShared; ++t)
             tiers += std::min<int64_t>(l.n_wfa, kTierDumpCap / pl.dump_stride[t]) *
                      pl.dump_stride[t];
         b += std::max(rings, tiers);

@@ -18,15 +18,16 @@
 // Tiers.  Work per pair grows with the square of its cost (most pairs are
 // cheap, most cells are in the few expensive ones), so a pair starts on the
 // smallest team and moves up when its interval outgrows the window:
-//   S  one warp per pair,      sixteen per block, W ~ 680  (x4 o6 e2)
-//   M  four warps per pair,    four per block,    W ~ 2,768
-//   L  sixteen warps per pair, one per block,     W ~ 11,088
+//   S   one warp per pair,      sixteen per block, W = 616  (x4 o6 e2)
+//   M   four warps per pair,    four per block,    W = 2,488
+//   L   eight warps per pair,   two per block,     W = 4,984
+//   XL  sixteen warps per pair, one per block,     W = 9,968
 // each in its own launch, one after another on the executor's stream.  A
 // pair whose next step would read or write outside its window is suspended:
 // the team writes its state (slot intervals, step, ring contents over the
 // live span) to a dump record in HBM and queues the pair for the next tier,
 // whose launch restores it into its larger window and continues from the
-// same step.  No cell is computed twice.  A pair that outgrows L, or whose
+// same step.  No cell is computed twice.  A pair that outgrows XL, or whose
 // rows could leave int16 (qlen + steps > 32767), runs from the start in the
 // G tier: sixteen warps per pair with int32 rings in a per-block region of
 // global memory large enough for any interval ([-max(qlen, rlen) - 3, ...]).
@@ -695,7 +696,7 @@ struct TierSpec {
     int32_t seq_bases;  // longest sequence copied to shared memory
 };
 // S, M, L tiers
-static const TierSpec kTiers[3] = {{1, 16, 2048}, {4, 4, 8192}, {16, 1, 32768}};
+static const TierSpec kTiers[kWfaShared] = {{1, 16, 2048}, {4, 4, 8192}, {8, 2, 16384}, {16, 1, 32768}};
 
 WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
 {
@@ -712,7 +713,7 @@ WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
     const int nslot = hm + 2 * hie;
     WfaTierPlan plan{};
     plan.nslot = nslot;
-    for (int t = 0; t < 3; ++t) {
+    for (int t = 0; t < kWfaShared; ++t) {
         const TierSpec &s = kTiers[t];
         const int64_t team_bytes = kTierBlockSmem / s.nteams;
         const int64_t seq_entries = 2 * ((s.seq_bases + 31) / 32);  // halves per sequence
@@ -729,13 +730,14 @@ WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
     }
     // G: int32 rings covering [-max(qlen, rlen) - 3, max(qlen, rlen) + 3]
     const int64_t lmax = std::max(qmax, rmax);
-    plan.W[3] = (int32_t)(((2 * lmax + 8) + 7) & ~int64_t(7));
-    plan.H[3] = (int32_t)(lmax + 3);
-    plan.seq_cap[3] = (int32_t)(2 * ((kTiers[2].seq_bases + 31) / 32));
-    plan.team_bytes[3] = 2 * (int64_t)plan.seq_cap[3] * 8;
-    plan.ring_bytes[3] = 0;
-    plan.usable[3] = true;
-    plan.gring_block_bytes = (int64_t)(nslot + 1) * plan.W[3] * 4;
+    constexpr int G = kWfaShared;
+    plan.W[G] = (int32_t)(((2 * lmax + 8) + 7) & ~int64_t(7));
+    plan.H[G] = (int32_t)(lmax + 3);
+    plan.seq_cap[G] = (int32_t)(2 * ((kTiers[G - 1].seq_bases + 31) / 32));
+    plan.team_bytes[G] = 2 * (int64_t)plan.seq_cap[G] * 8;
+    plan.ring_bytes[G] = 0;
+    plan.usable[G] = true;
+    plan.gring_block_bytes = (int64_t)(nslot + 1) * plan.W[G] * 4;
     return plan;
 }
 
@@ -774,11 +776,14 @@ cudaError_t launch_wfa_tier(const WfaTierPlan &pl, int tier, int grid, SeqView q
         return tier_launch<4, 4, int16_t, false>(pl, 1, grid, q, r, p, in, o, nullptr, out,
                                                  work, err_flag, st);
     case 2:
-        return tier_launch<16, 1, int16_t, false>(pl, 2, grid, q, r, p, in, o, nullptr, out,
+        return tier_launch<8, 2, int16_t, false>(pl, 2, grid, q, r, p, in, o, nullptr, out,
+                                                 work, err_flag, st);
+    case 3:
+        return tier_launch<16, 1, int16_t, false>(pl, 3, grid, q, r, p, in, o, nullptr, out,
                                                   work, err_flag, st);
     default:
-        return tier_launch<16, 1, int32_t, true>(pl, 3, grid, q, r, p, in, o, io.gring, out,
-                                                 work, err_flag, st);
+        return tier_launch<16, 1, int32_t, true>(pl, kWfaShared, grid, q, r, p, in, o, io.gring,
+                                                 out, work, err_flag, st);
     }
 }
 
