@@ -627,10 +627,11 @@ static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
 }
 
 // Tiered WFA (wfa_tiers.cu): every pair starts on the smallest team whose
-// launch still fills the GPU -- one warp (S) for large batches, four warps (M)
-// for up to 16 pairs per SM, eight (L) for up to two per SM, sixteen (XL) for
-// one, so a single long pair (the per-call drop-in) gets a whole SM -- and moves
-// up a tier when its wavefront outgrows the window; pairs that outgrow XL or need int32 rows
+// launch still fills the GPU -- one warp for large batches, four warps for up
+// to 16 pairs per SM, eight for up to two per SM, sixteen for one, so a single
+// long pair (the per-call drop-in) gets a whole SM -- and moves up a tier
+// (1, 2, 4, 8, 16 warps) when its wavefront outgrows the window; pairs that
+// outgrow the last or need int32 rows
 // finish in G.  One launch per tier from the first, in order on x.st; the
 // launches after the first take their pair count from the device.  With
 // GB2_FLAG_BATCHED the first tier's queue is ordered longest first.
@@ -640,7 +641,7 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
     const WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
     const int64_t sms = c->sm_count;
     constexpr int G = kWfaShared;  // the global-memory tier
-    int first = n <= sms ? 3 : (n <= 2 * sms ? 2 : (n <= 16 * sms ? 1 : 0));
+    int first = n <= sms ? 4 : (n <= 2 * sms ? 3 : (n <= 16 * sms ? 2 : 0));
     while (first < G && !pl.usable[first])
         ++first;
     auto next_of = [&](int t) {
@@ -694,7 +695,7 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
         list = (const int32_t *)x.queue.p;
         seg = (const int64_t *)x.seg.p;
     }
-    static const int teams_per_block[G + 1] = {16, 4, 2, 1, 1};
+    static const int teams_per_block[G + 1] = {16, 8, 4, 2, 1, 1};
     int prev = -1;  // the tier launched before t: its suspended pairs are t's entries
     for (int t = first; t <= G; ++t) {
         if (t < G && !pl.usable[t])
@@ -727,7 +728,7 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
             io.restart_n = q_n + kCounterStride * (G - 1);
         }
         io.gring = (int32_t *)x.scratch32.p;
-        // the tiers after S prune by the bound pass's costs
+        // the tiers after the first prune by the bound pass's costs
         io.ubound = (d_ub && t > 0) ? d_ub : nullptr;
         const int64_t per = teams_per_block[t];
         const int grid = (int)(t == first ? std::min<int64_t>(sms, (n + per - 1) / per) : sms);
@@ -737,8 +738,8 @@ static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, 
         prof_end(c, e0, x.st);
         c->launches += 1;
         if (t == 0 && d_ub && nt >= 0) {
-            // The bound pass: the pairs S suspended continue from their records
-            // (read, not consumed) on the S kernel inside a band of
+            // The bound pass: the pairs the one-warp tier suspended continue from
+            // their records (read, not consumed) on the one-warp kernel inside a band of
             // +-kWfaBoundBand diagonals around the line from diagonal 0 to the
             // target.  A hit there is a real alignment, so its cost bounds the
             // optimum from above; a pair the band cannot finish gets -1 (the
@@ -773,7 +774,7 @@ int wfa_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t 
     // the tiered kernels, unless the call asks for the naive baseline, a tuning
     // variant of the single-kernel design below, or the CIGAR pass's history sizes
     if (!(flags & GB2_FLAG_NAIVE) && ((flags >> 8) & 0xff) == 0 && !d_hist) {
-        // Batches with long pairs: for every pair the S tier suspends (the
+        // Batches with long pairs: for every pair the one-warp tier suspends (the
         // expensive ones), a bound pass finds the cost of its best alignment
         // inside a band of +-kWfaBoundBand diagonals around the line from
         // diagonal 0 to the target -- the cost of a real alignment, so no lower

@@ -109,11 +109,10 @@ cudaError_t launch_wfa(int variant, int block_warps, SeqView q, SeqView r, WfaPa
                        int64_t slot_width, int grid, int *err_flag, int64_t *work, int64_t *hist,
                        cudaStream_t st);
 
-// Tiered WFA (wfa_tiers.cu): tier 0 (S) one warp per pair, 1 (M) four warps,
-// 2 (L) eight warps, 3 (XL) sixteen warps, rings of W int16 per slot in shared
-// memory; tier kWfaShared (G) sixteen warps, int32 rings in global memory
-// covering every diagonal.
-constexpr int kWfaShared = 4;  // tiers with their rings in shared memory
+// Tiered WFA (wfa_tiers.cu): tiers 0..4 align a pair with 1, 2, 4, 8 and 16
+// warps, rings of W int16 per slot in shared memory; tier kWfaShared (G)
+// sixteen warps, int32 rings in global memory covering every diagonal.
+constexpr int kWfaShared = 5;  // tiers with their rings in shared memory
 struct WfaTierPlan {
     int nslot;
     int32_t W[kWfaShared + 1], H[kWfaShared + 1];  // window per slot row; element of diagonal 0

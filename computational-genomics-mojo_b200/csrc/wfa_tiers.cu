@@ -18,16 +18,17 @@
 // Tiers.  Work per pair grows with the square of its cost (most pairs are
 // cheap, most cells are in the few expensive ones), so a pair starts on the
 // smallest team and moves up when its interval outgrows the window:
-//   S   one warp per pair,      sixteen per block, W = 616  (x4 o6 e2)
-//   M   four warps per pair,    four per block,    W = 2,488
-//   L   eight warps per pair,   two per block,     W = 4,984
-//   XL  sixteen warps per pair, one per block,     W = 9,968
+//   T1   one warp per pair,      sixteen per block, W = 616  (x4 o6 e2)
+//   T2   two warps per pair,     eight per block,   W = 1,240
+//   T4   four warps per pair,    four per block,    W = 2,488
+//   T8   eight warps per pair,   two per block,     W = 4,984
+//   T16  sixteen warps per pair, one per block,     W = 9,968
 // each in its own launch, one after another on the executor's stream.  A
 // pair whose next step would read or write outside its window is suspended:
 // the team writes its state (slot intervals, step, ring contents over the
 // live span) to a dump record in HBM and queues the pair for the next tier,
 // whose launch restores it into its larger window and continues from the
-// same step.  No cell is computed twice.  A pair that outgrows XL, or whose
+// same step.  No cell is computed twice.  A pair that outgrows T16, or whose
 // rows could leave int16 (qlen + steps > 32767), runs from the start in the
 // G tier: sixteen warps per pair with int32 rings in a per-block region of
 // global memory large enough for any interval ([-max(qlen, rlen) - 3, ...]).
@@ -696,7 +697,7 @@ struct TierSpec {
     int32_t seq_bases;  // longest sequence copied to shared memory
 };
 // S, M, L tiers
-static const TierSpec kTiers[kWfaShared] = {{1, 16, 2048}, {4, 4, 8192}, {8, 2, 16384}, {16, 1, 32768}};
+static const TierSpec kTiers[kWfaShared] = {{1, 16, 2048}, {2, 8, 4096}, {4, 4, 8192}, {8, 2, 16384}, {16, 1, 32768}};
 
 WfaTierPlan wfa_tier_plan(const WfaParams &p, int64_t qmax, int64_t rmax)
 {
@@ -773,13 +774,16 @@ cudaError_t launch_wfa_tier(const WfaTierPlan &pl, int tier, int grid, SeqView q
         return tier_launch<1, 16, int16_t, false>(pl, 0, grid, q, r, p, in, o, nullptr, out,
                                                   work, err_flag, st);
     case 1:
-        return tier_launch<4, 4, int16_t, false>(pl, 1, grid, q, r, p, in, o, nullptr, out,
+        return tier_launch<2, 8, int16_t, false>(pl, 1, grid, q, r, p, in, o, nullptr, out,
                                                  work, err_flag, st);
     case 2:
-        return tier_launch<8, 2, int16_t, false>(pl, 2, grid, q, r, p, in, o, nullptr, out,
+        return tier_launch<4, 4, int16_t, false>(pl, 2, grid, q, r, p, in, o, nullptr, out,
                                                  work, err_flag, st);
     case 3:
-        return tier_launch<16, 1, int16_t, false>(pl, 3, grid, q, r, p, in, o, nullptr, out,
+        return tier_launch<8, 2, int16_t, false>(pl, 3, grid, q, r, p, in, o, nullptr, out,
+                                                 work, err_flag, st);
+    case 4:
+        return tier_launch<16, 1, int16_t, false>(pl, 4, grid, q, r, p, in, o, nullptr, out,
                                                   work, err_flag, st);
     default:
         return tier_launch<16, 1, int32_t, true>(pl, kWfaShared, grid, q, r, p, in, o, io.gring,
