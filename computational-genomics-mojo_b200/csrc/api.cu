@@ -638,8 +638,13 @@ static int wfa_block_warps(int64_t qmax, int64_t rmax, int64_t n, int variant)
 static int wfa_tiers(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t rmax,
                      const WfaParams &p, int64_t n, int32_t *d_out, int flags, int32_t *d_ub)
 {
-    const WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
+    WfaTierPlan pl = wfa_tier_plan(p, qmax, rmax);
     const int64_t sms = c->sm_count;
+    // The two-warp tier pays off when the batch leaves it enough pairs: on the
+    // long-pair workload it saved 5 ms at 100,000 pairs and 1.4 ms at 40,000, and
+    // cost 0.5 ms at 20,000 and 1.3 ms at 10,000 (one more launch in the chain).
+    if (n < kWfaTwoWarpMinPairsPerSm * sms)
+        pl.usable[1] = false;
     constexpr int G = kWfaShared;  // the global-memory tier
     int first = n <= sms ? 4 : (n <= 2 * sms ? 3 : (n <= 16 * sms ? 2 : 0));
     while (first < G && !pl.usable[first])

@@ -31,6 +31,8 @@ constexpr int64_t kTierDumpCap = 1ll << 30;    // bytes of suspended-pair record
 // WFA bound pass: batches whose longest sequence has at least kWfaBoundMinLen
 // bases run it, over a band of +-kWfaBoundBand diagonals
 constexpr int64_t kWfaBoundMinLen = 1024;
+// WFA: batches of fewer pairs per SM than this skip the two-warp tier
+constexpr int64_t kWfaTwoWarpMinPairsPerSm = 160;
 constexpr int32_t kWfaBoundBand = 64;
 
 // Grow-only device buffer.
