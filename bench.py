@@ -452,6 +452,12 @@ def our_arm(args, dist: Dist):
         print(json.dumps(line), flush=True)
 
 
+class _PinnedOwner:
+    """Keeps page-locked host blocks alive as long as the arrays that use them."""
+    def __init__(self):
+        self._pinned_blocks = []
+
+
 def _time_steps(dev, fn, steps, warmup):
     """Device time (ms) per step of fn() on the library stream, L2 flushed between."""
     for _ in range(warmup):
@@ -472,6 +478,8 @@ def extras(args, dev, peak_ops, hbm_peak):
     import oracle as O
     from genomics_b200 import AlignConfig, WFAConfig, synth
     from genomics_b200._lib import FLAG_NAIVE, FLAG_NO_PRUNE
+    from genomics_b200.core import pinned_empty
+    from genomics_b200.device import SW_RESULT_DTYPE
     O.build()
     threads = os.cpu_count() or 1
     out = {}
@@ -480,11 +488,19 @@ def extras(args, dev, peak_ops, hbm_peak):
     cfg = AlignConfig(*SCORING, 32)
     cells = synth.sw_cells(q, bands)
     dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
-    tb = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=True), 3, 2)
-    tp = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=False), 3, 2)
-    tn = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=False,
-                                                flags=FLAG_NAIVE), 2, 1)
-    res_b = np.array(dev.sw_banded(dq, dr, cfg, bands=bands, batched=True))
+    # the per-pair bands in and the results out through page-locked host arrays, as the
+    # headline's results are (a pageable array adds a host copy inside the timed region)
+    own = _PinnedOwner()
+    pbands = pinned_empty(bands.size, np.int32, own)
+    pbands[:] = bands
+    sw_out = pinned_empty(bands.size * SW_RESULT_DTYPE.itemsize, np.uint8, own).view(SW_RESULT_DTYPE)
+    tb = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True,
+                                                out=sw_out), 3, 2)
+    tp = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=False,
+                                                out=sw_out), 3, 2)
+    tn = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=False,
+                                                flags=FLAG_NAIVE, out=sw_out), 2, 1)
+    res_b = np.array(dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True, out=sw_out))
     m = 3000
     t0 = time.perf_counter()
     qp, _, qo, ql = q.arrays()
@@ -522,7 +538,8 @@ def extras(args, dev, peak_ops, hbm_peak):
     # whole mixed batch (one class after another), then the batch timed again
     from genomics_b200 import autotune
     table = autotune.tune(dev, dq, dr, sw_cfg=cfg, reps=3, pair_bands=bands)
-    tt = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=bands, batched=True), 3, 2)
+    tt = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True,
+                                                out=sw_out), 3, 2)
     out["mixed_sw_200k"]["autotuned"] = {
         "table": table["sw"], "candidates_ms": table["measurements"],
         "tuned_on": "the whole 200,000-pair mixed call, one band class after another",
@@ -536,24 +553,26 @@ def extras(args, dev, peak_ops, hbm_peak):
     wcfg = WFAConfig(4, 6, 2, me)
     dq, dr = dev.upload_batch(q, with_nmask=False), dev.upload_batch(r, with_nmask=False)
     n = 100_000
+    wout = pinned_empty(n, np.int32, own)
     dev.stats_reset()
-    tb = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True), 2, 1)
+    tb = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True, out=wout), 2, 1)
     wcells = dev.stats()["work_units"] // 3
     wres = np.array(dev.wfa_affine(dq, dr, wcfg, batched=True))
     # the envelope the algorithm defines (every diagonal the sources reach, no bound
     # pruning): the algorithmic work the roofline counts, and that path's time
     dev.stats_reset()
     tnp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True,
-                                                  flags=FLAG_NO_PRUNE), 1, 1)
+                                                  flags=FLAG_NO_PRUNE, out=wout), 1, 1)
     ecells = dev.stats()["work_units"] // 2
-    tp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False), 2, 1)
+    tp = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False, out=wout), 2, 1)
     tn = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=False,
-                                                 flags=FLAG_NAIVE), 1, 1)
+                                                 flags=FLAG_NAIVE, out=wout), 1, 1)
     # the single-kernel design with rings in global memory (tuning variant 5: five
     # 4-warp blocks per SM, length-sorted queue) for comparison
-    tg = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True, flags=5 << 8), 1, 1)
+    tg = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, wcfg, batched=True, flags=5 << 8,
+                                                 out=wout), 1, 1)
     w200 = WFAConfig(4, 6, 2, 200)
-    t200 = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, w200, batched=True), 2, 1)
+    t200 = _time_steps(dev, lambda: dev.wfa_affine(dq, dr, w200, batched=True, out=wout), 2, 1)
     c200 = dev.wfa_affine(dq, dr, w200, batched=True)
     wbytes = q.packed.nbytes + r.packed.nbytes + 20 * n
     qp, _, qo, ql = q.arrays()

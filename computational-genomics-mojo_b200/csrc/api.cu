@@ -545,12 +545,19 @@ int sw_validate(gb2_ctx *c, const gb2_sw_cfg *cfg, const int32_t *bands, int64_t
         return set_err(c, GB2_EINVAL, "n_pairs < 0");
     int32_t maxb = cfg->band_width;
     if (bands) {
-        maxb = 0;
+        // one branch-free pass (it vectorises); the offending pair only on error
+        int32_t lo = 0, hi = 0;
         for (int64_t i = 0; i < n; ++i) {
-            if (bands[i] < 0)
-                return set_err(c, GB2_EINVAL, "band of pair %lld is negative", (long long)i);
-            maxb = std::max(maxb, bands[i]);
+            lo = std::min(lo, bands[i]);
+            hi = std::max(hi, bands[i]);
         }
+        if (lo < 0) {
+            int64_t i = 0;
+            while (bands[i] >= 0)
+                ++i;
+            return set_err(c, GB2_EINVAL, "band of pair %lld is negative", (long long)i);
+        }
+        maxb = hi;
     } else if (cfg->band_width < 0) {
         return set_err(c, GB2_EINVAL, "band_width < 0");
     }
