@@ -483,6 +483,28 @@ def extras(args, dev, peak_ops, hbm_peak):
     O.build()
     threads = os.cpu_count() or 1
     out = {}
+    # each band class alone: the 1,000,000 reads of the headline workload with one band
+    # for every pair (bands 16/32 take the narrow-key packed kernel, 64/128 the wide-key one)
+    q1, r1, _, _ = synth.generate(1, 1_000_000)
+    d1q, d1r = dev.upload_batch(q1, with_nmask=False), dev.upload_batch(r1, with_nmask=False)
+    own1 = _PinnedOwner()
+    out1 = pinned_empty(q1.count * SW_RESULT_DTYPE.itemsize, np.uint8, own1).view(SW_RESULT_DTYPE)
+    classes = {}
+    for band in (16, 32, 64, 128):
+        cfg_b = AlignConfig(*SCORING, band)
+        tcb = _time_steps(dev, lambda: dev.sw_banded(d1q, d1r, cfg_b, batched=True, out=out1),
+                          5, 3)
+        cells_b = synth.sw_cells(q1, band)
+        classes[f"band_{band}"] = {"gcups": round(cells_b / tcb / 1e6, 1), "ms": round(tcb, 3),
+                                   "kernel": f"sw_pack16_kernel<{band}, "
+                                             f"{'narrow' if band <= 32 else 'wide'} keys>"}
+    out["sw_band_classes_1M_reads"] = {
+        "workload": "the 1,000,000 reads of the headline workload (150 vs 200 bp, "
+                    "+2/-4/-4/-2), one band for every pair, resident, results into "
+                    "page-locked memory",
+        **classes}
+    d1q.close()
+    d1r.close()
     # mixed-band SW: 200,000 pairs, 100-2,000 bp, bands {16,32,64,128}, N runs
     q, r, bands, _ = synth.generate(3, 200_000)
     cfg = AlignConfig(*SCORING, 32)
