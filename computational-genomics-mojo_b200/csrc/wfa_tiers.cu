@@ -238,6 +238,26 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
 // hi} at 0, lane j's {M slot j lo, hi, I/D slot j lo, hi} at int 32 + 4j, and
 // from byte kDumpHeader the nslot ring rows over [span lo, span hi], each
 // span elements of int16.
+//
+// The shared-memory tiers write the rows with one bulk asynchronous copy per
+// row (cp.async.bulk, shared to global, no multicast), which needs both
+// addresses and the size in whole 16-byte units.  So the span is the live
+// span widened outward to diagonals whose window positions H + k are
+// multiples of 8: the window's rows start on 16 bytes (W is a multiple of 8,
+// the ring 16-byte aligned) and hold positions [0, W), so the widened span
+// stays inside the row; outside every slot's interval a row holds NEG, so the
+// extra elements are NEG.  Records lie whole multiples of 256 bytes apart and
+// the rows at kDumpHeader + j * span * 2 with span a multiple of 8; the
+// alignment is checked when a record is written (an element copy otherwise).  The larger window a
+// record is restored into holds the widened span too (its H and W - H are no
+// smaller), where the extra NEGs land on NEG.
+__device__ __forceinline__ void bulk_row_to_global(void *dst, const void *src_smem,
+                                                   uint32_t bytes)
+{
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(src_smem);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(dst), "r"(s), "r"(bytes) : "memory");
+}
 struct DumpOut {
     uint8_t *base;      // records of dump_stride bytes
     int64_t stride;
@@ -433,6 +453,10 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                     }
                     l0 = __reduce_min_sync(FULL, l0);
                     h0 = __reduce_max_sync(FULL, h0);
+                    if (R16 && l0 <= h0) {  // widen to 16-byte units of the window rows
+                        l0 -= (H + l0) & 7;
+                        h0 += 7 - ((H + h0) & 7);
+                    }
                     if (tt == 0) {
                         hd[0] = (int32_t)sp;
                         hd[1] = ms;
@@ -449,10 +473,31 @@ __device__ __forceinline__ int32_t tier_pair(const SeqView &q, const SeqView &r,
                     const int32_t span = h0 - l0 + 1;
                     if (span > 0) {
                         int16_t *dst = reinterpret_cast<int16_t *>(rec + kDumpHeader);
-                        const int32_t total = w.nslot * span;
-                        for (int32_t i = tt; i < total; i += TW) {
-                            const int32_t j = i / span, kk = i - j * span;
-                            dst[i] = (int16_t)slot(j)[l0 + kk];
+                        // alignment as derived above, checked (the same on every thread
+                        // of the team): the element copy below otherwise
+                        const bool bulk =
+                            R16 && (((uintptr_t)dst & 15u) == 0) && ((W & 7) == 0) &&
+                            ((__cvta_generic_to_shared(slot(0) + l0) & 15u) == 0);
+                        if (bulk) {
+                            // every thread orders its ring writes before the async
+                            // proxy's reads, then one thread hands the rows to the
+                            // copy engine and waits for them before the team can
+                            // reuse the window (the next pair starts with a barrier)
+                            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                            team.sync();
+                            if (tt == 0) {
+                                for (int j = 0; j < w.nslot; ++j)
+                                    bulk_row_to_global(dst + (int64_t)j * span, slot(j) + l0,
+                                                       (uint32_t)span * 2u);
+                                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                                asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                            }
+                        } else {
+                            const int32_t total = w.nslot * span;
+                            for (int32_t i = tt; i < total; i += TW) {
+                                const int32_t j = i / span, kk = i - j * span;
+                                dst[i] = (int16_t)slot(j)[l0 + kk];
+                            }
                         }
                     }
                 }
