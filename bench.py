@@ -517,9 +517,9 @@ def extras(args, dev, peak_ops, hbm_peak):
     pbands[:] = bands
     sw_out = pinned_empty(bands.size * SW_RESULT_DTYPE.itemsize, np.uint8, own).view(SW_RESULT_DTYPE)
     tb = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True,
-                                                out=sw_out), 3, 2)
+                                                out=sw_out), 10, 5)
     tp = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=False,
-                                                out=sw_out), 3, 2)
+                                                out=sw_out), 10, 5)
     tn = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=False,
                                                 flags=FLAG_NAIVE, out=sw_out), 2, 1)
     res_b = np.array(dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True, out=sw_out))
@@ -561,7 +561,7 @@ def extras(args, dev, peak_ops, hbm_peak):
     from genomics_b200 import autotune
     table = autotune.tune(dev, dq, dr, sw_cfg=cfg, reps=3, pair_bands=bands)
     tt = _time_steps(dev, lambda: dev.sw_banded(dq, dr, cfg, bands=pbands, batched=True,
-                                                out=sw_out), 3, 2)
+                                                out=sw_out), 10, 5)
     out["mixed_sw_200k"]["autotuned"] = {
         "table": table["sw"], "candidates_ms": table["measurements"],
         "tuned_on": "the whole 200,000-pair mixed call, one band class after another",
