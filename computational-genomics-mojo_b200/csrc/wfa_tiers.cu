@@ -240,7 +240,7 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
 // span elements of int16.
 //
 // The shared-memory tiers write the rows with one bulk asynchronous copy per
-// row (cp.async.bulk, shared to global, no multicast), which needs both
+// row (cp.async.bulk from this CTA's shared memory to global), which needs both
 // addresses and the size in whole 16-byte units.  So the span is the live
 // span widened outward to diagonals whose window positions H + k are
 // multiples of 8: the window's rows start on 16 bytes (W is a multiple of 8,
