@@ -409,7 +409,13 @@ int sw_core(gb2_ctx *c, Exec &x, SeqView qv, SeqView rv, int64_t qmax, int64_t r
         return GB2_OK;
     }
     const bool pack = pi.pack_ok && !force_literal && !(flags & GB2_FLAG_INT32);
-    const bool wide = pack && pi.wide_ok;
+    // Wide keys: a small batch leaves most SMs idle and its longest pair's row loop
+    // is the call's critical path, which the int32 kernels with the most lanes per
+    // pair (var_of) shorten; one thread per pair of the packed kernel does not (2,000
+    // mixed-band pairs: 2.4 ms against 4.4; one pair per call: about 1,800 against
+    // 1,100 pairs/s).  GB2_FLAG_PACKED keeps the packed kernel for small batches too.
+    const bool wide =
+        pack && pi.wide_ok && (n > kSwSmallBatch || (flags & GB2_FLAG_PACKED) != 0);
     const int64_t hbound = (int64_t)match_pos * (std::min(qmax, rmax) + 1);
     const bool pack_lengths = hbound <= kPackHmax;
     const bool wide_lengths = hbound <= kWideHmax;

@@ -36,6 +36,7 @@ FLAG_GENERIC = 0x4
 FLAG_GRAPH = 0x8  # capture resident calls into a CUDA graph and replay it
 FLAG_NAIVE = 0x10  # baseline: one thread block per pair, input order, no planning
 FLAG_NO_PRUNE = 0x20  # WFA: no bound pass, every reachable diagonal (same results)
+FLAG_PACKED = 0x40  # SW: the wide-key packed kernel for small batches too (same results)
 
 
 class SwCfg(ctypes.Structure):

@@ -88,6 +88,10 @@ typedef struct gb2_batch gb2_batch;
 #define GB2_FLAG_NO_PRUNE 0x20 /* gb2_wfa_affine: skip the bound pass (a banded WFA whose
                                   costs bound the optimum from above) and the exact pass's
                                   pruning by it; results are the same either way */
+#define GB2_FLAG_PACKED 0x40  /* gb2_sw_banded*: take the packed int16 kernel with wide keys
+                                  for batches of at most 16,384 pairs too (by default they
+                                  run the int32 kernels with the most lanes per pair, which
+                                  finish a small batch sooner); results are the same */
 /* Tuning fields (0 = the library's choice): bits 8-15 select a kernel
  * variant; bits 16-23 set how many chunks the *_host entry points split a
  * batch into for their copy/compute pipeline. */

@@ -7,7 +7,7 @@ import pytest
 
 import genomics_b200 as G
 from genomics_b200 import AlignConfig, SequenceBatch, synth
-from genomics_b200._lib import FLAG_GENERIC, FLAG_INT32, GenomicsError
+from genomics_b200._lib import FLAG_GENERIC, FLAG_INT32, FLAG_PACKED, GenomicsError
 
 pytestmark = pytest.mark.gpu
 
@@ -199,10 +199,11 @@ def test_packed_int16_path_matches_int32_and_oracle(device, oracle, band):
 @pytest.mark.parametrize("band", [16, 32, 64, 128])
 def test_packed_wide_keys_match_int32_and_oracle(device, oracle, band):
     """Pairs whose scores pass 511 (the narrow keys' limit) but stay within
-    match * (min(qlen, rlen) + 1) <= 4094 take the packed kernel with group keys;
-    GB2_FLAG_INT32 forces the int32 register kernels.  Both equal the oracle,
-    including first-maximum ties across groups and halves and rows past either
-    end."""
+    match * (min(qlen, rlen) + 1) <= 4094 take the packed kernel with group keys
+    (GB2_FLAG_PACKED: these batches are small enough to run the int32 kernels by
+    default, which must give the same results); GB2_FLAG_INT32 forces the int32
+    register kernels.  All equal the oracle, including first-maximum ties across
+    groups and halves and rows past either end."""
     rng = random.Random(band * 13)
     q, r = _random_pairs(rng, 600, 2000, "ACGTN")
     # similar pairs reach large scores; repeats make equal maxima in many columns
@@ -214,8 +215,9 @@ def test_packed_wide_keys_match_int32_and_oracle(device, oracle, band):
                     AlignConfig(3, -2, -6, -1, band), AlignConfig(2, -8, -2, -1, band)):
             ref = oracle_sw(oracle, qq, rr, cfg)
             for batched in (False, True):
-                assert_same(device.sw_banded(qq, rr, cfg, batched=batched), ref,
-                            f"{cfg} wide packed batched={batched}")
+                assert_same(device.sw_banded(qq, rr, cfg, batched=batched, flags=FLAG_PACKED),
+                            ref, f"{cfg} wide packed batched={batched}")
+            assert_same(device.sw_banded(qq, rr, cfg), ref, f"{cfg} default")
             assert_same(device.sw_banded(qq, rr, cfg, flags=FLAG_INT32), ref, f"{cfg} int32")
 
 
@@ -235,8 +237,9 @@ def test_packed_wide_key_bounds(device, oracle):
     ref = oracle_sw(oracle, q, r, CFG0, bands=b)
     assert (ref[0] > 4000).any()
     for batched in (False, True):
-        assert_same(device.sw_banded(q, r, CFG0, bands=b, batched=batched), ref,
-                    f"bounds batched={batched}")
+        for flags in (0, FLAG_PACKED):
+            assert_same(device.sw_banded(q, r, CFG0, bands=b, batched=batched, flags=flags),
+                        ref, f"bounds batched={batched} flags={flags}")
 
 
 def test_variants_agree(device, oracle):
