@@ -46,6 +46,23 @@ def test_library_loads_and_binding_covers_header(built_lib):
     assert L.gb2_strerror(-5) == b"input outside the exact integer range"
 
 
+def test_flag_and_status_constants_match_header():
+    """The Python binding's flag bits and status codes are the header's."""
+    from genomics_b200 import _lib
+    text = open(HEADER).read()
+    defines = {name: int(val, 0) for name, val in
+               re.findall(r"#define (GB2_(?:FLAG_[A-Z0-9_]+|E[A-Z]+|OK))\s+\(?(-?(?:0x)?[0-9a-fA-F]+)",
+                          text)}
+    flags = {k: v for k, v in defines.items() if k.startswith("GB2_FLAG_")}
+    assert "GB2_FLAG_PACKED" in flags and len(flags) >= 8
+    for name, val in flags.items():
+        assert getattr(_lib, name[len("GB2_"):]) == val, name
+    assert len(set(flags.values())) == len(flags)  # no two flags share a bit
+    for name, val in defines.items():
+        if not name.startswith("GB2_FLAG_"):
+            assert getattr(_lib, name) == val, name
+
+
 def test_struct_layouts_match_header(built_lib):
     from genomics_b200 import _lib
     assert ctypes.sizeof(_lib.SwCfg) == 20
