@@ -160,6 +160,35 @@ def test_wfa_envelope_equals_statement_for_statement(oracle):
         assert a == b, (q, r, x, o, e, me)
 
 
+def test_wfa_envelope_equals_statement_for_statement_long(oracle):
+    """Pairs of 300-3,000 bases at 1-10% divergence: the live-envelope form (what the
+    long-pair parity checks use) equals the statement-for-statement form at the exact
+    cost, one below it (-1) and above it."""
+    rng = random.Random(1500)
+    for _ in range(60):
+        q = _rand_seq(rng, rng.randint(300, 3000))
+        r = list(q)
+        for _k in range(int(len(q) * rng.uniform(0.01, 0.10))):
+            op = rng.random()
+            pos = rng.randint(0, len(r) - 1)
+            if op < 0.7:
+                r[pos] = rng.choice("ACGT")
+            elif op < 0.85:
+                r.insert(pos, rng.choice("ACGT"))
+            elif len(r) > 1:
+                del r[pos]
+        r = "".join(r)
+        x, o, e = rng.choice([(4, 6, 2), (1, 1, 1), (3, 5, 1), (6, 8, 3), (2, 0, 2)])
+        cost = oracle.wfa_affine(q, r, x, o, e, 4 * (len(q) + len(r)), envelope=True)
+        assert cost >= 0
+        for me in (cost, cost - 1, cost + 17):
+            if me < 0:
+                continue
+            a = oracle.wfa_affine(q, r, x, o, e, me)
+            b = oracle.wfa_affine(q, r, x, o, e, me, envelope=True)
+            assert a == b == (cost if me >= cost else -1), (len(q), len(r), x, o, e, me, a, b)
+
+
 def test_wfa_batch_driver_matches_single(oracle):
     from genomics_b200 import synth
     q, r, _, _ = synth.generate(2, 40, seed=5)
