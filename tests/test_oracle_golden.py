@@ -135,6 +135,51 @@ def test_sw_matches_naive_restatement(oracle):
         assert (got[0], got[3], got[4]) == (s, qi, ri), (q, r, prm, b)
 
 
+def _nw_naive(q, r, m, mm, go, ge, b):
+    """Banded NW in (row, reference position) coordinates, the oracle's intended
+    semantics of align_cpu.mojo:312-377 written without band offsets: row 0 reads
+    the initial band row (indexed like row 0, :330-337), later rows the previous
+    row's cells; skipped and out-of-band cells are NEG; the end cell is
+    (qlen - 1, rlen - 1) when it lies in the band (:365-368)."""
+    NEG = -1000000
+    qn, rn = len(q), len(r)
+
+    def init(x):  # the initial band row at reference position x
+        return NEG if x < 0 else (0 if x == 0 else go + x * ge)
+
+    H = {}
+    for qi in range(qn):
+        for ri in range(max(0, qi - b), min(rn, qi + b + 1)):
+            sub = m if _base(q, qi) == _base(r, ri) else mm
+            if qi == 0:
+                hd = init(ri)
+                hu = init(ri + 1) if ri + 1 <= b else NEG
+            else:
+                hd = H.get((qi - 1, ri - 1), NEG) if ri - 1 >= qi - 1 - b else NEG
+                hu = H.get((qi - 1, ri), NEG) if ri <= qi - 1 + b else NEG
+            hl = H.get((qi, ri - 1), NEG) if ri - 1 >= qi - b else NEG
+            H[(qi, ri)] = max(hd + sub, hu + go + ge, hl + go + ge)
+    if qn == 0:  # no row ran: the end cell reads the initial row at offset rlen - 1 + b + 1
+        off = (rn - 1) - (0 - 1) + b
+        return init(off - b) if 0 <= off < 2 * b + 1 else NEG
+    if abs((rn - 1) - (qn - 1)) > b:
+        return NEG
+    return H.get((qn - 1, rn - 1), NEG)
+
+
+def test_nw_matches_naive_restatement(oracle):
+    rng = random.Random(13)
+    for _ in range(400):
+        q = _rand_seq(rng, rng.randint(0, 40), "ACGTN")
+        r = _rand_seq(rng, rng.randint(0, 40), "ACGTN")
+        if rng.random() < 0.5 and q:
+            r = q[: rng.randint(0, len(q))] + _rand_seq(rng, rng.randint(0, 8))
+        b = rng.randint(0, 12)
+        prm = (rng.randint(0, 4), -rng.randint(0, 5), -rng.randint(0, 6), -rng.randint(0, 3))
+        got = oracle.nw_banded(q, r, *prm, band=b)
+        assert got[0] == _nw_naive(q, r, *prm, b), (q, r, prm, b)
+
+
 def test_wfa_envelope_equals_statement_for_statement(oracle):
     rng = random.Random(11)
     for _ in range(400):
