@@ -70,6 +70,56 @@ def test_wfa_cigar_known_answers(oracle, known):
         assert _cigar_len(cig, "=XD") == len(r)
 
 
+def _cigar_walk_ok(cigar, q, r):
+    """'=' runs pair equal bases, 'X' runs unequal ones, I consumes the query, D the
+    reference, and the walk ends at both ends."""
+    i = j = cnt = 0
+    for ch in cigar:
+        if ch.isdigit():
+            cnt = cnt * 10 + int(ch)
+            continue
+        for _ in range(cnt):
+            if ch in "=X":
+                if i >= len(q) or j >= len(r) or (q[i] == r[j]) != (ch == "="):
+                    return False
+                i += 1
+                j += 1
+            elif ch == "I":
+                i += 1
+            else:
+                j += 1
+        cnt = 0
+    return i == len(q) and j == len(r)
+
+
+def test_wfa_cigar_properties_on_random_pairs(oracle):
+    """For random pairs and penalties: the CIGAR's cost equals the cost, which equals
+    wfa_affine's; the CIGAR walks both sequences with '=' on equal and 'X' on unequal
+    bases; past max_error the cost is -1 and the CIGAR empty."""
+    rng = random.Random(380)
+    for _ in range(300):
+        q = _rand_seq(rng, rng.randint(0, 120))
+        r = list(q)
+        for _k in range(rng.randint(0, 12)):
+            op, pos = rng.random(), rng.randint(0, max(len(r) - 1, 0))
+            if op < 0.5 and r:
+                r[pos] = rng.choice("ACGT")
+            elif op < 0.75:
+                r.insert(pos, rng.choice("ACGT"))
+            elif r:
+                del r[pos]
+        r = "".join(r) if rng.random() < 0.9 else _rand_seq(rng, rng.randint(0, 60))
+        x, o, e = rng.randint(1, 6), rng.randint(0, 8), rng.randint(1, 4)
+        me = rng.choice([10, 60, 300])
+        cost, cig = oracle.wfa_cigar(q, r, x, o, e, me)
+        assert cost == oracle.wfa_affine(q, r, x, o, e, me)
+        if cost < 0:
+            assert cig == ""
+            continue
+        assert _cigar_cost(cig, x, o, e) == cost, (q, r, x, o, e, cig)
+        assert _cigar_walk_ok(cig, q, r), (q, r, cig)
+
+
 def test_encoding_known_answers(oracle, known):
     enc = known["encoding"]
     for c, v in enc["ascii_to_2bit"]["cases"]:
