@@ -354,8 +354,8 @@ __device__ __forceinline__ uint32_t pack16_cells(uint32_t (&Hr)[B + 1], const ui
     // hide the latency of the left-to-right chain through a row: there the
     // H update is grouped so that only the 3-way max waits on the left
     // neighbour (two dependent instructions per register instead of three).
-    // Measured on 1,000,000 reads: band 128 2,723 -> 2,896 GCUPS, band 64
-    // 3,613 -> 3,654; the narrow bands 16 and 32 (20 warps per SM) are 4%
+    // Measured on 1,000,000 reads: band 128 2,723 -> 2,901 GCUPS, band 64
+    // 3,613 -> 3,655; the narrow bands 16 and 32 (20 warps per SM) are 4%
     // faster with the other grouping.
     constexpr bool SHORT_CHAIN = B >= 64;
     const uint32_t SENT = 0x0000C000u;

@@ -248,9 +248,9 @@ __device__ __forceinline__ void ext_u(const SeqWin &qs, int32_t qlen, const SeqW
 // stays inside the row; outside every slot's interval a row holds NEG, so the
 // extra elements are NEG.  Records lie whole multiples of 256 bytes apart and
 // the rows at kDumpHeader + j * span * 2 with span a multiple of 8; the
-// alignment is checked when a record is written (an element copy otherwise).  The larger window a
-// record is restored into holds the widened span too (its H and W - H are no
-// smaller), where the extra NEGs land on NEG.
+// alignment is checked when a record is written (an element copy otherwise).
+// The larger window a record is restored into holds the widened span too (its
+// H and W - H are no smaller), where the extra NEGs land on NEG.
 __device__ __forceinline__ void bulk_row_to_global(void *dst, const void *src_smem,
                                                    uint32_t bytes)
 {
